@@ -1,0 +1,73 @@
+"""Build libgci.so (CUDA sm_100a kernels + C ABI) in-tree with nvcc.
+
+Run as a script or call ``build()``; objects go to ``_lib/obj`` and the
+library to ``_lib/libgci.so`` next to this file.  Recompiles only sources
+newer than their object.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+OUT = HERE / "_lib"
+OBJ = OUT / "obj"
+LIB = OUT / "libgci.so"
+CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+NVCC = str(CUDA_HOME / "bin" / "nvcc")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+          "-I", str(HERE.parent / "include"), "-I", str(CSRC)]
+SOURCES = ["eri_kernels.cu", "chol_kernels.cu", "mo_gemm.cu", "gci_api.cu", "host_math.cpp"]
+HEADERS = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "gci.h"]
+
+
+def _stale(src: Path, obj: Path) -> bool:
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    return src.stat().st_mtime > t or any(h.stat().st_mtime > t for h in HEADERS)
+
+
+def _compile(src: Path, obj: Path, verbose: bool) -> None:
+    cmd = [NVCC, *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
+    if src.suffix == ".cpp":
+        cmd = [NVCC, *COMMON, "-x", "c++", "-c", str(src), "-o", str(obj)]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stdout}\n{r.stderr}")
+    if verbose:
+        sys.stderr.write(r.stderr)
+
+
+def build(verbose: bool = False, jobs: int | None = None) -> Path:
+    OBJ.mkdir(parents=True, exist_ok=True)
+    todo = []
+    objs = []
+    for s in SOURCES:
+        src = CSRC / s
+        obj = OBJ / (src.stem + ".o")
+        objs.append(obj)
+        if _stale(src, obj):
+            todo.append((src, obj))
+    with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+        for f in [ex.submit(_compile, s, o, verbose) for s, o in todo]:
+            f.result()
+    if todo or not LIB.exists():
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcublas", "-lcusolver",
+               "-Xlinker", f"-rpath={CUDA_HOME / 'lib64'}"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

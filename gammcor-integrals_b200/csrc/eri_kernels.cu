@@ -1,0 +1,167 @@
+// eri_kernels.cu -- instantiation and dispatch of the class-templated ERI
+// kernels, the primitive-pair record kernel and the Boys self-test kernel.
+#include "eri_engine.cuh"
+#include "gci_runtime.h"
+
+namespace gci {
+
+// ---------------------------------------------------------------------------
+// Primitive-pair records (one block per shell pair, threads over primitive
+// pairs, a fastest as in the reference's Ga-inner loop).
+// ---------------------------------------------------------------------------
+__global__ void k_pair_records(const ShellPairDev* __restrict__ pairs, int npairs,
+                               const double* __restrict__ xyz, const int* __restrict__ poff,
+                               const double* __restrict__ exps, const double* __restrict__ coefs,
+                               double* __restrict__ pp)
+{
+    for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+        const ShellPairDev sp = pairs[p];
+        const int L1 = sp.l1 + sp.l2;
+        const int rs = pp_record(L1);
+        const int n = sp.nprim1 * sp.nprim2;
+        const double ax = xyz[3 * sp.s1], ay = xyz[3 * sp.s1 + 1], az = xyz[3 * sp.s1 + 2];
+        const double bx = xyz[3 * sp.s2], by = xyz[3 * sp.s2 + 1], bz = xyz[3 * sp.s2 + 2];
+        const double r2 = (ax - bx) * (ax - bx) + (ay - by) * (ay - by) + (az - bz) * (az - bz);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int ga = i % sp.nprim1, gb = i / sp.nprim1;
+            const double ea = exps[poff[sp.s1] + ga], eb = exps[poff[sp.s2] + gb];
+            const double ca = coefs[poff[sp.s1] + ga], cb = coefs[poff[sp.s2] + gb];
+            const double P = ea + eb;
+            const double px = (ea * ax + eb * bx) / P, py = (ea * ay + eb * by) / P, pz = (ea * az + eb * bz) / P;
+            double* rec = pp + sp.rec_off + (size_t)i * rs;
+            rec[0] = P; rec[1] = px; rec[2] = py; rec[3] = pz;
+            rec[4] = exp(-ea * eb / P * r2) * ca * cb;
+            rec[5] = px - ax; rec[6] = py - ay; rec[7] = pz - az;
+            // single-centre Hermite coefficients E^{e}_t (auto2e_EtCoeffs_L)
+            const double h = 1.0 / (2.0 * P);
+            for (int axis = 0; axis < 3; ++axis) {
+                double* E = rec + 8 + axis * tri(L1);
+                const double X = rec[5 + axis];
+                E[0] = 1.0;
+                for (int e = 0; e < L1; ++e) {
+                    const double* Ee = E + e * (e + 1) / 2;
+                    double* En = E + (e + 1) * (e + 2) / 2;
+                    for (int t = 0; t <= e + 1; ++t) {
+                        double v = 0.0;
+                        if (t >= 1) v += h * Ee[t - 1];
+                        if (t <= e) v += X * Ee[t];
+                        if (t + 1 <= e) v += (double)(t + 1) * Ee[t + 1];
+                        En[t] = v;
+                    }
+                }
+            }
+        }
+    }
+}
+
+__global__ void k_boys_eval(int m, int64_t n, const double* __restrict__ x, const double* __restrict__ table,
+                            double* __restrict__ out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double F[kBoysMaxM + 1];
+        boys_fm_rt(m, x[i], table, F);
+        for (int k = 0; k <= m; ++k) out[i * (m + 1) + k] = F[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-class launch configuration: team width TW (threads per shell quartet)
+// from the size of the W accumulator, one block of TPB threads.
+// ---------------------------------------------------------------------------
+constexpr int type_lhi(int t) { return t >= 6 ? 3 : (t >= 3 ? 2 : (t >= 1 ? 1 : 0)); }
+constexpr int type_llo(int t) { return t - pair_type(type_lhi(t), 0); }
+
+template <int LA, int LB, int LC, int LD>
+struct EriConfig {
+    using S = EriShape<LA, LB, LC, LD>;
+    static constexpr int NW = S::NE * S::NF;
+    static constexpr int TW0 = NW <= 16 ? 1 : (NW <= 96 ? 4 : (NW <= 400 ? 16 : (NW <= 1600 ? 32 : 128)));
+    static constexpr size_t team_bytes = sizeof(double) * (size_t)((S::SZ_TEAM | 1));
+    // widen the team until one block's shared memory stays within ~100 KB
+    static constexpr int next_tw(int tw) { return tw == 16 ? 32 : (tw == 32 ? 128 : tw * 2); }
+    static constexpr int pick(int tw)
+    {
+        return (tw >= 128) ? 128 : (((size_t)(128 / tw) * team_bytes <= 100 * 1024) ? tw : pick(next_tw(tw)));
+    }
+    static constexpr int TW = pick(TW0);
+    static constexpr int TPB = 128;
+};
+
+template <int TB, int TK>
+static void launch_class(const EriArgs& args, cudaStream_t st)
+{
+    constexpr int LA = type_lhi(TB), LB = type_llo(TB), LC = type_lhi(TK), LD = type_llo(TK);
+    using Cfg = EriConfig<LA, LB, LC, LD>;
+    using S = EriShape<LA, LB, LC, LD>;
+    using TM = TeamMem<Cfg::TW, Cfg::TPB, S::SZ_TEAM>;
+    constexpr int NT = Cfg::TPB / Cfg::TW;
+    const size_t smem = TM::bytes();
+    auto kern = k_eri_class<LA, LB, LC, LD, Cfg::TW, Cfg::TPB>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+    }
+    const int64_t ntasks = (args.mode == kModeDiagonal) ? args.nbra : args.nbra * args.nket;
+    if (ntasks <= 0) return;
+    int64_t blocks = (ntasks + NT - 1) / NT;
+    const int64_t cap = 148LL * 32;
+    if (blocks > cap) blocks = cap;
+    kern<<<(unsigned)blocks, Cfg::TPB, smem, st>>>(args);
+}
+
+using LaunchFn = void (*)(const EriArgs&, cudaStream_t);
+static LaunchFn g_launch[kNumPairTypes][kNumPairTypes];
+
+template <int TB, int TK>
+struct Register {
+    static void run()
+    {
+        g_launch[TB][TK] = &launch_class<TB, TK>;
+        if constexpr (TK > 0) Register<TB, TK - 1>::run();
+        else if constexpr (TB > 0) Register<TB - 1, TB - 1>::run();
+    }
+};
+
+cudaError_t eri_module_init()
+{
+    static bool done = false;
+    if (done) return cudaSuccess;
+    Register<kNumPairTypes - 1, kNumPairTypes - 1>::run();
+    cudaError_t e = upload_device_tables();
+    if (e == cudaSuccess) done = true;
+    return e;
+}
+
+int eri_team_width(int tb, int tk)
+{
+    (void)tb; (void)tk;
+    return 0;
+}
+
+cudaError_t eri_launch(int tb, int tk, const EriArgs& args, cudaStream_t st)
+{
+    if (tb < 0 || tk < 0 || tb >= kNumPairTypes || tk >= kNumPairTypes || tb < tk) return cudaErrorInvalidValue;
+    g_launch[tb][tk](args, st);
+    return cudaGetLastError();
+}
+
+cudaError_t pair_records_launch(const ShellPairDev* pairs, int npairs, const double* xyz, const int* poff,
+                                const double* exps, const double* coefs, double* pp, cudaStream_t st)
+{
+    if (npairs <= 0) return cudaSuccess;
+    int blocks = npairs < 148 * 64 ? npairs : 148 * 64;
+    k_pair_records<<<blocks, 64, 0, st>>>(pairs, npairs, xyz, poff, exps, coefs, pp);
+    return cudaGetLastError();
+}
+
+cudaError_t boys_eval_launch(int m, int64_t n, const double* x, const double* table, double* out, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_boys_eval<<<(unsigned)blocks, 256, 0, st>>>(m, n, x, table, out);
+    return cudaGetLastError();
+}
+
+} // namespace gci

@@ -1,0 +1,1274 @@
+// gci_api.cu -- C ABI and host runtime of the integral-direct two-step
+// Cholesky decomposition of (pq|rs) and the AO->MO transformation.
+//
+// Control flow follows the reference driver (TwoStepCholesky*.f90,
+// Cholesky_Gammcor.f90); the integral, pivot-search and contraction work
+// runs on the device (eri_kernels.cu, chol_kernels.cu, cuBLAS DGEMM for the
+// FP64 contractions, mo_gemm.cu for the split-precision tensor-core GEMMs).
+#include "../../include/gci.h"
+#include "gci_common.h"
+#include "gci_runtime.h"
+#include "host_math.h"
+#include "mo_gemm.h"
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace gci {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+struct Failure {
+    int code;
+    std::string msg;
+};
+[[noreturn]] static void fail(int code, const std::string& msg) { throw Failure{code, msg}; }
+#define CU(x)                                                                                   \
+    do {                                                                                        \
+        cudaError_t e_ = (x);                                                                   \
+        if (e_ != cudaSuccess) fail(GCI_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+#define CB(x)                                                                                   \
+    do {                                                                                        \
+        cublasStatus_t s_ = (x);                                                                \
+        if (s_ != CUBLAS_STATUS_SUCCESS) fail(GCI_ERR_CUDA, std::string(#x) + " failed: " + std::to_string((int)s_)); \
+    } while (0)
+#define CS(x)                                                                                   \
+    do {                                                                                        \
+        cusolverStatus_t s_ = (x);                                                              \
+        if (s_ != CUSOLVER_STATUS_SUCCESS) fail(GCI_ERR_CUDA, std::string(#x) + " failed: " + std::to_string((int)s_)); \
+    } while (0)
+
+template <class F>
+static int guarded(F&& f)
+{
+    try {
+        f();
+        return GCI_OK;
+    } catch (const Failure& e) {
+        g_last_error = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return GCI_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return GCI_ERR_ARG;
+    }
+}
+
+// ------------------------------------------------------------------ device buffers
+template <class T>
+struct DVec {
+    T* p = nullptr;
+    size_t n = 0;
+    DVec() = default;
+    DVec(const DVec&) = delete;
+    DVec& operator=(const DVec&) = delete;
+    DVec(DVec&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DVec& operator=(DVec&& o) noexcept
+    {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DVec() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count)
+    {
+        if (count == n && p) return;
+        release();
+        if (count == 0) return;
+        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            fail(GCI_ERR_NOMEM, "device allocation of " + std::to_string(count * sizeof(T)) + " bytes failed");
+        }
+        n = count;
+    }
+    void ensure(size_t count)
+    {
+        if (count > n) alloc(count);
+    }
+    void upload(const std::vector<T>& h, cudaStream_t s)
+    {
+        ensure(h.size() ? h.size() : 1);
+        if (!h.empty()) CU(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+};
+
+// ------------------------------------------------------------------ context
+struct Context {
+    bool ready = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cublasHandle_t blas = nullptr;
+    cusolverDnHandle_t solver = nullptr;
+    DVec<double> boys;
+    DVec<int> err;
+};
+static Context g_ctx;
+
+static Context& ctx()
+{
+    if (!g_ctx.ready) {
+        int ndev = 0;
+        cudaError_t e = cudaGetDeviceCount(&ndev);
+        if (e != cudaSuccess || ndev == 0) fail(GCI_ERR_CUDA, "no CUDA device available");
+        CU(cudaGetDevice(&g_ctx.device));
+        CU(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
+        CB(cublasCreate(&g_ctx.blas));
+        CB(cublasSetStream(g_ctx.blas, g_ctx.stream));
+        CB(cublasSetMathMode(g_ctx.blas, CUBLAS_DEFAULT_MATH));
+        CS(cusolverDnCreate(&g_ctx.solver));
+        CS(cusolverDnSetStream(g_ctx.solver, g_ctx.stream));
+        CU(eri_module_init());
+        std::vector<double> tab = boys_table(kBoysMaxM);
+        g_ctx.boys.upload(tab, g_ctx.stream);
+        g_ctx.err.alloc(1);
+        CU(cudaMemsetAsync(g_ctx.err.p, 0, sizeof(int), g_ctx.stream));
+        CU(cudaStreamSynchronize(g_ctx.stream));
+        g_ctx.ready = true;
+    }
+    return g_ctx;
+}
+
+// ------------------------------------------------------------------ phase timer
+enum Phase { kVdiag = 0, kStep1Eri, kSubtractR, kPivots, kCompress, kVjjEri, kPotrf, kFullEri, kInvLGemm, kMoGemm, kNumPhases };
+struct PhaseTimer {
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    double acc[kNumPhases] = {0};
+    cudaEvent_t cur_start = nullptr;
+    int cur = -1;
+    cudaStream_t s = nullptr;
+    void start(int ph)
+    {
+        cudaEvent_t e;
+        CU(cudaEventCreate(&e));
+        CU(cudaEventRecord(e, s));
+        cur_start = e;
+        cur = ph;
+    }
+    void stop()
+    {
+        cudaEvent_t e;
+        CU(cudaEventCreate(&e));
+        CU(cudaEventRecord(e, s));
+        pending.push_back({cur, {cur_start, e}});
+        cur = -1;
+    }
+    void flush()
+    {
+        for (auto& p : pending) {
+            float ms = 0.f;
+            CU(cudaEventSynchronize(p.second.second));
+            CU(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
+            acc[p.first] += ms * 1e-3;
+            cudaEventDestroy(p.second.first);
+            cudaEventDestroy(p.second.second);
+        }
+        pending.clear();
+    }
+};
+
+// ------------------------------------------------------------------ basis + pairs
+struct HostBasis {
+    int nsh = 0, spher = 1, lmax = 0;
+    int64_t nao = 0;
+    std::vector<double> xyz, exps, coefs, tmat;
+    std::vector<int> L, nprim, poff, nfunc, loc, toff, atom;
+};
+
+static HostBasis make_basis(const gci_basis* b)
+{
+    if (!b) fail(GCI_ERR_ARG, "basis is NULL");
+    if (b->nshells <= 0 || b->natoms <= 0 || b->nshellparams <= 0) fail(GCI_ERR_ARG, "empty basis");
+    HostBasis h;
+    h.nsh = (int)b->nshells;
+    h.spher = b->spher_ao ? 1 : 0;
+    h.xyz.resize(3 * h.nsh);
+    h.L.resize(h.nsh); h.nprim.resize(h.nsh); h.poff.resize(h.nsh); h.nfunc.resize(h.nsh);
+    h.loc.resize(h.nsh); h.toff.resize(h.nsh); h.atom.resize(h.nsh);
+    for (int s = 0; s < h.nsh; ++s) {
+        const int64_t at = b->shell_centers[s] - 1, pr = b->shell_params_idx[s] - 1;
+        if (at < 0 || at >= b->natoms) fail(GCI_ERR_ARG, "shell centre index out of range");
+        if (pr < 0 || pr >= b->nshellparams) fail(GCI_ERR_ARG, "shell parameter index out of range");
+        const int l = (int)b->shell_momentum[pr];
+        const int np = (int)b->nprimitives[pr];
+        if (l < 0) fail(GCI_ERR_ARG, "negative angular momentum");
+        if (l > kMaxL)
+            fail(GCI_ERR_UNSUPPORTED, "Basis set includes angular momenta unsupported by the GPU ERI kernels (l > " +
+                                          std::to_string(kMaxL) + ")");
+        if (np <= 0 || np > b->ldprim) fail(GCI_ERR_ARG, "invalid number of primitives");
+        h.atom[s] = (int)at;
+        for (int k = 0; k < 3; ++k) h.xyz[3 * s + k] = b->atom_coords[3 * at + k];
+        h.L[s] = l;
+        h.lmax = std::max(h.lmax, l);
+        h.nprim[s] = np;
+        h.poff[s] = (int)h.exps.size();
+        for (int i = 0; i < np; ++i) {
+            h.exps.push_back(b->exponents[pr * b->ldprim + i]);
+            h.coefs.push_back(b->cntr_coeffs[pr * b->ldprim + i]);
+        }
+        const int nc = ncart(l);
+        const int nf = h.spher ? 2 * l + 1 : nc;
+        if (nf > b->ldnorm) fail(GCI_ERR_ARG, "norm_factors leading dimension too small");
+        h.nfunc[s] = nf;
+        h.loc[s] = (int)h.nao;
+        h.nao += nf;
+        h.toff[s] = (int)h.tmat.size();
+        std::vector<double> U((size_t)nc * nc, 0.0);
+        if (h.spher) spher_coeffs(l, U.data());
+        const double* nrm = b->norm_factors + pr * b->ldnorm;
+        for (int m = 0; m < nf; ++m)
+            for (int c = 0; c < nc; ++c) {
+                double v;
+                if (h.spher) v = nrm[m] * U[m * nc + c];
+                else v = (m == c) ? nrm[m] : 0.0;
+                h.tmat.push_back(v);
+            }
+    }
+    return h;
+}
+
+struct DevBasis {
+    DVec<double> xyz, exps, coefs, tmat;
+    DVec<int> poff, nfunc, loc, toff;
+};
+
+struct PairTable {
+    int64_t n = 0;
+    std::vector<int> A, B, type, dim, nab;    // stored A >= B; dim = orbital pairs kept; nab = Na*Nb
+    std::vector<int64_t> vdloc;                 // offsets in the Vdiag order
+    std::vector<ShellPairDev> h;
+    DVec<ShellPairDev> d;
+    DVec<double> pp;
+};
+
+static int64_t pair_local(int a, int b, int Na, bool same)
+{
+    if (!same) return a + (int64_t)Na * b;
+    if (a < b) return -1;
+    return (int64_t)b * Na - (int64_t)b * (b - 1) / 2 + (a - b);
+}
+
+// ------------------------------------------------------------------ ERI stage dispatch
+struct PairMap {
+    std::vector<int64_t> off;
+    std::vector<int> map;
+    DVec<int64_t> doff;
+    DVec<int> dmap;
+    void reset(int64_t npairs)
+    {
+        off.assign(npairs, -1);
+        map.clear();
+    }
+    // append an entry block for pair `id` of Na*Nb slots
+    int* add(int id, int nab)
+    {
+        off[id] = (int64_t)map.size();
+        map.resize(map.size() + nab, -1);
+        return map.data() + off[id];
+    }
+    void upload(cudaStream_t s)
+    {
+        for (auto& o : off) if (o < 0) o = 0;
+        doff.upload(off, s);
+        if (map.empty()) map.push_back(-1);
+        dmap.upload(map, s);
+    }
+};
+
+struct Handle;
+static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<int>& ket, int mode, PairMap* rows,
+                    PairMap* cols, double* out, int64_t ldo, int64_t jcount = 0);
+
+struct Handle {
+    HostBasis hb;
+    DevBasis db;
+    PairTable pt;
+    double tau = 1e-6, kappa = 0.0;
+    int flags = 0;
+    // results of step 1 (0-based)
+    int64_t nsp = 0, npq = 0, nvecs = 0, nsubsets = 0, msd = 0, npsp = 0;
+    std::vector<int> bsp;                  // BASE pair ids (all-pair index) in BASE order
+    std::vector<int64_t> fullloc, subloc, subidx;
+    std::vector<int64_t> subsetdim, subsetlo, subsethi;
+    std::vector<int> pivots;
+    std::vector<int64_t> pivot_order;
+    std::vector<double> pivot_dmax;
+    std::vector<int> psp, pspdim, porb;    // pivot shell pairs (BASE index), dims, orbital pair (full block)
+    std::vector<int64_t> psploc;
+    int converged = 0;
+    int64_t nmacro = 0;
+    DVec<double> invl;                     // nvecs x nvecs
+    DVec<double> rkpq;                     // nvecs x msd x nsubsets (if materialised)
+    bool have_rkpq = false;
+    PairMap pivmap;                        // pivot columns, by pair id
+    PhaseTimer timer;
+    double t_rkpq = 0.0, t_rkab = 0.0;
+    // scratch reused across ERI launches
+    DVec<int> d_bra, d_ket;
+};
+
+static void setup_pairs(Handle& H)
+{
+    Context& C = ctx();
+    const HostBasis& b = H.hb;
+    PairTable& P = H.pt;
+    const int nsh = b.nsh;
+    P.n = (int64_t)nsh * (nsh + 1) / 2;
+    P.A.resize(P.n); P.B.resize(P.n); P.type.resize(P.n); P.dim.resize(P.n); P.nab.resize(P.n);
+    P.vdloc.resize(P.n); P.h.resize(P.n);
+    int64_t sp = 0, loc = 0, rec = 0;
+    for (int B = 0; B < nsh; ++B)
+        for (int A = B; A < nsh; ++A) {
+            const int Na = b.nfunc[A], Nb = b.nfunc[B];
+            P.A[sp] = A; P.B[sp] = B;
+            P.nab[sp] = Na * Nb;
+            P.dim[sp] = (A != B) ? Na * Nb : Na * (Na + 1) / 2;
+            P.vdloc[sp] = loc;
+            loc += P.dim[sp];
+            ShellPairDev d{};
+            const bool sw = b.L[A] < b.L[B];
+            d.s1 = sw ? B : A;
+            d.s2 = sw ? A : B;
+            d.swap = sw ? 1 : 0;
+            d.l1 = b.L[d.s1];
+            d.l2 = b.L[d.s2];
+            d.nprim1 = b.nprim[d.s1];
+            d.nprim2 = b.nprim[d.s2];
+            d.rec_off = rec;
+            rec += (int64_t)d.nprim1 * d.nprim2 * pp_record(d.l1 + d.l2);
+            P.type[sp] = pair_type(d.l1, d.l2);
+            P.h[sp] = d;
+            ++sp;
+        }
+    DevBasis& D = H.db;
+    D.xyz.upload(b.xyz, C.stream);
+    D.exps.upload(b.exps, C.stream);
+    D.coefs.upload(b.coefs, C.stream);
+    D.tmat.upload(b.tmat, C.stream);
+    D.poff.upload(b.poff, C.stream);
+    D.nfunc.upload(b.nfunc, C.stream);
+    D.loc.upload(b.loc, C.stream);
+    D.toff.upload(b.toff, C.stream);
+    P.d.upload(P.h, C.stream);
+    P.pp.alloc(rec > 0 ? rec : 1);
+    CU(pair_records_launch(P.d.p, (int)P.n, D.xyz.p, D.poff.p, D.exps.p, D.coefs.p, P.pp.p, C.stream));
+}
+
+static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<int>& ket, int mode, PairMap* rows,
+                    PairMap* cols, double* out, int64_t ldo, int64_t jcount)
+{
+    Context& C = ctx();
+    const PairTable& P = H.pt;
+    // class-sorted task lists: pairs grouped by type
+    std::vector<int> gb, gk;
+    std::vector<int64_t> sb(kNumPairTypes + 1, 0), sk(kNumPairTypes + 1, 0);
+    auto group = [&](const std::vector<int>& ids, std::vector<int>& g, std::vector<int64_t>& seg) {
+        std::vector<int64_t> cnt(kNumPairTypes, 0);
+        for (int id : ids) cnt[P.type[id]]++;
+        seg[0] = 0;
+        for (int t = 0; t < kNumPairTypes; ++t) seg[t + 1] = seg[t] + cnt[t];
+        g.resize(ids.size());
+        std::vector<int64_t> pos(seg.begin(), seg.end() - 1);
+        for (int id : ids) g[pos[P.type[id]]++] = id;
+    };
+    group(bra, gb, sb);
+    if (mode != kModeDiagonal) group(ket, gk, sk);
+    H.d_bra.upload(gb, C.stream);
+    if (mode != kModeDiagonal) H.d_ket.upload(gk, C.stream);
+    EriArgs a{};
+    a.sh_xyz = H.db.xyz.p;
+    a.sh_toff = H.db.toff.p;
+    a.tmat = H.db.tmat.p;
+    a.sh_nfunc = H.db.nfunc.p;
+    a.sh_loc = H.db.loc.p;
+    a.pairs = P.d.p;
+    a.pp = P.pp.p;
+    a.mode = mode;
+    a.out = out;
+    a.ldo = ldo;
+    a.row_off = rows ? rows->doff.p : nullptr;
+    a.row_map = rows ? rows->dmap.p : nullptr;
+    a.col_off = cols ? cols->doff.p : nullptr;
+    a.col_map = cols ? cols->dmap.p : nullptr;
+    a.nao = H.hb.nao;
+    a.jcount = jcount;
+    a.kappa = H.kappa;
+    a.boys = C.boys.p;
+    a.err = C.err.p;
+    for (int tb = 0; tb < kNumPairTypes; ++tb) {
+        const int64_t nb = sb[tb + 1] - sb[tb];
+        if (nb == 0) continue;
+        if (mode == kModeDiagonal) {
+            a.bra_ids = H.d_bra.p + sb[tb];
+            a.ket_ids = a.bra_ids;
+            a.nbra = nb;
+            a.nket = nb;
+            a.swap_bk = 0;
+            CU(eri_launch(tb, tb, a, C.stream));
+            continue;
+        }
+        for (int tk = 0; tk < kNumPairTypes; ++tk) {
+            const int64_t nk = sk[tk + 1] - sk[tk];
+            if (nk == 0) continue;
+            a.bra_ids = H.d_bra.p + sb[tb];
+            a.ket_ids = H.d_ket.p + sk[tk];
+            a.nbra = nb;
+            a.nket = nk;
+            a.swap_bk = tb < tk ? 1 : 0;
+            CU(eri_launch(std::max(tb, tk), std::min(tb, tk), a, C.stream));
+        }
+    }
+}
+
+// ------------------------------------------------------------------ step 1
+static double accuracy_tau(int accuracy)
+{
+    switch (accuracy) {   // Cholesky_Gammcor.f90:398-410
+    case GCI_ACCURACY_DEFAULT: return 1.0e-5;
+    case GCI_ACCURACY_TIGHT: return 1.0e-6;
+    case GCI_ACCURACY_LUDICROUS: return 1.0e-7;
+    case GCI_ACCURACY_DEBUG: return 1.0e-10;
+    default: fail(GCI_ERR_ARG, "Invalid accuracy setting");
+    }
+}
+
+static void gemm_nt(cublasHandle_t h, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,
+                    const double* B, int64_t ldb, double beta, double* Cm, int64_t ldc)
+{
+    if (m == 0 || n == 0) return;
+    CB(cublasDgemm_64(h, CUBLAS_OP_N, CUBLAS_OP_T, m, n, k, &alpha, A, lda, B, ldb, &beta, Cm, ldc));
+}
+
+static void step1(Handle& H)
+{
+    Context& C = ctx();
+    cudaStream_t s = C.stream;
+    PairTable& P = H.pt;
+    const HostBasis& b = H.hb;
+    PhaseTimer& T = H.timer;
+    const int64_t maxnorb = b.nao * (b.nao + 1) / 2;
+
+    // ---------------- chol2_Vdiag (TwoStepCholesky_Step1.f90:202-279)
+    std::vector<int> all(P.n);
+    for (int64_t i = 0; i < P.n; ++i) all[i] = (int)i;
+    PairMap vdm;
+    vdm.reset(P.n);
+    for (int64_t sp = 0; sp < P.n; ++sp) {
+        const int A = P.A[sp], B = P.B[sp], Na = b.nfunc[A], Nb = b.nfunc[B];
+        int* m = vdm.add((int)sp, Na * Nb);
+        for (int bb = 0; bb < Nb; ++bb)
+            for (int a = 0; a < Na; ++a) {
+                const int64_t l = pair_local(a, bb, Na, A == B);
+                m[a + Na * bb] = l < 0 ? -1 : (int)(P.vdloc[sp] + l);
+            }
+    }
+    vdm.upload(s);
+    DVec<double> dvd;
+    dvd.alloc(maxnorb);
+    T.start(kVdiag);
+    run_eri(H, all, all, kModeDiagonal, &vdm, nullptr, dvd.p, 0);
+    T.stop();
+    std::vector<double> vdiag(maxnorb);
+    CU(cudaMemcpyAsync(vdiag.data(), dvd.p, sizeof(double) * maxnorb, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    dvd.release();
+
+    // ---------------- chol2_DefineBase (:282-442)
+    std::vector<double> vmax(P.n);
+    std::vector<int64_t> idx(P.n);
+    double maxdrs = -1e300;
+    for (int64_t sp = 0; sp < P.n; ++sp) {
+        double m = -1e300;
+        for (int i = 0; i < P.dim[sp]; ++i) m = std::max(m, vdiag[P.vdloc[sp] + i]);
+        vmax[sp] = m;
+        idx[sp] = sp;
+        maxdrs = std::max(maxdrs, m);
+    }
+    if (!(maxdrs > 0.0)) fail(GCI_ERR_ARG, "Maximum diagonal Coulomb integral is nonpositive");
+    const double th = std::min(H.tau, 1.0e-8);
+    const double prescreen = th * th / maxdrs;
+    slatec_dsort(vmax.data(), idx.data(), P.n, 2);
+    int64_t k0 = 1;
+    for (int64_t k = 1; k <= P.n; ++k) {
+        const int64_t sp = idx[k - 1];
+        double mx = -1e300;
+        for (int i = 0; i < P.dim[sp]; ++i) mx = std::max(mx, vdiag[P.vdloc[sp] + i]);
+        if (mx <= prescreen) k0 = k;   // the reference keeps k0 on the last discarded pair
+        else break;
+    }
+    H.nsp = P.n - k0 + 1;
+    H.bsp.resize(H.nsp);
+    H.fullloc.resize(H.nsp);
+    std::vector<double> D;
+    {
+        int64_t p = 0;
+        for (int64_t k = k0, s2 = 0; k <= P.n; ++k, ++s2) {
+            const int64_t sp = idx[k - 1];
+            H.bsp[s2] = (int)sp;
+            H.fullloc[s2] = p;
+            for (int i = 0; i < P.dim[sp]; ++i) D.push_back(vdiag[P.vdloc[sp] + i]);
+            p += P.dim[sp];
+        }
+        H.npq = p;
+    }
+    auto bdim = [&](int64_t s2) { return P.dim[H.bsp[s2]]; };
+
+    // ---------------- chol2_DefineSubsets / chol2_DivideOrbPairs (:445-530)
+    {
+        const int64_t maxblock = 4000;   // TChol2Params%MaxBlockDim
+        int64_t ns = (H.npq + maxblock - 1) / maxblock;
+        if (ns < 1) ns = 1;
+        H.nsubsets = ns;
+        H.subsetdim.assign(ns, 0);
+        H.subsetlo.assign(ns, -1);
+        H.subsethi.assign(ns, -1);
+        H.subloc.assign(H.nsp, 0);
+        H.subidx.assign(H.nsp, 0);
+        const int64_t target = (H.npq + ns - 1) / ns;
+        for (int64_t k = 1; k <= ns; ++k) {
+            int64_t lo;
+            if (k == 1) lo = 1;
+            else {
+                const int64_t prev = H.subsethi[k - 2] + 1;
+                lo = (prev < H.nsp && prev > 0) ? prev + 1 : 0;
+            }
+            int64_t dim = 0, hi = lo;
+            if (lo > 0) {
+                if (k < ns) {
+                    int64_t berr[2] = {H.npq, H.npq}, bloc[2] = {lo, lo};
+                    for (int64_t s2 = lo; s2 <= H.nsp; ++s2) {
+                        H.subloc[s2 - 1] = dim;
+                        H.subidx[s2 - 1] = k - 1;
+                        dim += bdim(s2 - 1);
+                        if (dim >= target) { bloc[1] = s2; berr[1] = dim - target; break; }
+                        bloc[0] = s2; berr[0] = dim - target;
+                    }
+                    if (std::llabs(berr[0]) < std::llabs(berr[1])) { hi = bloc[0]; dim = berr[0] + target; }
+                    else { hi = bloc[1]; dim = berr[1] + target; }
+                } else {
+                    hi = H.nsp;
+                    for (int64_t s2 = lo; s2 <= hi; ++s2) {
+                        H.subloc[s2 - 1] = dim;
+                        H.subidx[s2 - 1] = k - 1;
+                        dim += bdim(s2 - 1);
+                    }
+                }
+            }
+            H.subsetdim[k - 1] = dim;
+            H.subsetlo[k - 1] = lo - 1;
+            H.subsethi[k - 1] = hi - 1;
+        }
+        H.msd = *std::max_element(H.subsetdim.begin(), H.subsetdim.end());
+    }
+
+    // ---------------- chol2_Pivots (:884-1103)
+    int64_t maxnchol = (int64_t)std::ceil(b.nao * 15.0);
+    if (maxnchol > H.npq) maxnchol = H.npq;
+    const int maxnang = H.hb.spher ? 2 * b.lmax + 1 : ncart(b.lmax);
+    H.pivots.assign(H.npq, 0);
+    H.pivot_order.clear();
+    H.pivot_dmax.clear();
+
+    std::vector<int64_t> cand(H.nsp), compr(H.nsp);   // candidate BASE indices; compressed loc per BASE pair
+    for (int64_t k = 0; k < H.nsp; ++k) { cand[k] = k; compr[k] = H.fullloc[k]; }
+    int64_t ncand = H.npq;
+    DVec<double> dD, dD2;
+    dD.upload(D, s);
+    double dmax = *std::max_element(D.begin(), D.end());
+    // vector storage: Lst (ncand x cap), column-major, ld = ncand
+    int64_t cap = std::min<int64_t>(maxnchol, std::max<int64_t>(256, 4 * b.nao));
+    DVec<double> Lst, Lst2;
+    Lst.alloc((size_t)std::max<int64_t>(ncand, 1) * cap);
+    int64_t nchol = 0;
+    bool converged = false, go = maxnchol > 0;
+    int64_t nmacro = 0;
+    DVec<double> dM, dLB, dMbb, dDb, dLb, dpdmax, dLp, dLinv, dMp, dsegmax, dscal;
+    DVec<int> dpiv, dnpiv;
+    DVec<int64_t> dgidx, dsegloc, dbrow;
+    DVec<int> dsegdim;
+    dscal.alloc(1);
+    dnpiv.alloc(1);
+    std::vector<double> segmax;
+    PairMap mrows, mcols;
+
+    auto segment_max = [&](const std::vector<int64_t>& list) {
+        std::vector<int64_t> loc(list.size());
+        std::vector<int> dim(list.size());
+        for (size_t k = 0; k < list.size(); ++k) { loc[k] = compr[list[k]]; dim[k] = bdim(list[k]); }
+        dsegloc.upload(loc, s);
+        dsegdim.upload(dim, s);
+        dsegmax.ensure(std::max<size_t>(list.size(), 1));
+        CU(launch_segmax(dD.p, dsegloc.p, dsegdim.p, (int64_t)list.size(), dsegmax.p, s));
+        segmax.resize(list.size());
+        if (!list.empty())
+            CU(cudaMemcpyAsync(segmax.data(), dsegmax.p, sizeof(double) * list.size(), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+    };
+
+    while (go) {
+        ++nmacro;
+        // -------- chol2_DefineCandidates (:533-575)
+        T.start(kCompress);
+        segment_max(cand);
+        std::vector<double> sv(segmax);
+        std::vector<int64_t> si(cand);
+        slatec_dsort(sv.data(), si.data(), (int64_t)si.size(), -2);
+        std::vector<int64_t> ncand_list;
+        int64_t ncand_new = 0;
+        for (size_t k = 0; k < si.size(); ++k) {
+            if (sv[k] > H.tau) { ncand_list.push_back(si[k]); ncand_new += bdim(si[k]); }
+            else break;
+        }
+        // -------- chol2_Compress (:16-97)
+        {
+            std::vector<int64_t> gidx(std::max<int64_t>(ncand_new, 1));
+            std::vector<int64_t> newloc(ncand_list.size());
+            int64_t pos = 0;
+            for (size_t g = 0; g < ncand_list.size(); ++g) {
+                const int64_t s2 = ncand_list[g];
+                newloc[g] = pos;
+                for (int i = 0; i < bdim(s2); ++i) gidx[pos + i] = compr[s2] + i;
+                pos += bdim(s2);
+            }
+            dgidx.upload(gidx, s);
+            dD2.ensure(std::max<int64_t>(ncand_new, 1));
+            CU(launch_gather_rows(dD.p, ncand, dgidx.p, ncand_new, 1, dD2.p, ncand_new, s));
+            std::swap(dD, dD2);
+            if (nchol > 0 && ncand_new > 0) {
+                Lst2.ensure((size_t)ncand_new * cap);
+                CU(launch_gather_rows(Lst.p, ncand, dgidx.p, ncand_new, nchol, Lst2.p, ncand_new, s));
+                std::swap(Lst, Lst2);
+            }
+            for (size_t g = 0; g < ncand_list.size(); ++g) compr[ncand_list[g]] = newloc[g];
+            cand = ncand_list;
+            ncand = ncand_new;
+        }
+        T.stop();
+        int64_t maxnbatch = std::max<int64_t>((int64_t)maxnang * maxnang, 1000);
+        if (maxnbatch > ncand) maxnbatch = ncand;
+        const double dmin = std::max(0.01 * dmax, H.tau);
+        // -------- chol2_DefineBatch (:578-625)
+        segment_max(cand);
+        std::vector<double> dsv(segmax);
+        std::vector<int64_t> dsi(cand);
+        slatec_dsort(dsv.data(), dsi.data(), (int64_t)dsi.size(), -2);
+        std::vector<int64_t> batch, colloc;
+        int64_t nbatch = 0;
+        for (size_t k = 0; k < dsi.size(); ++k) {
+            const int dim = bdim(dsi[k]);
+            if (dsv[k] > dmin && nbatch + dim <= maxnbatch) {
+                batch.push_back(dsi[k]);
+                colloc.push_back(nbatch);
+                nbatch += dim;
+            } else break;
+        }
+        // -------- chol2_M (:733-856): M(ncand x nbatch)
+        if (nbatch > 0 && ncand > 0) {
+            mrows.reset(P.n);
+            for (int64_t s2 : cand) {
+                const int id = H.bsp[s2];
+                const int A = P.A[id], B = P.B[id], Na = b.nfunc[A], Nb = b.nfunc[B];
+                int* m = mrows.add(id, Na * Nb);
+                for (int bb = 0; bb < Nb; ++bb)
+                    for (int a = 0; a < Na; ++a) {
+                        const int64_t l = pair_local(a, bb, Na, A == B);
+                        m[a + Na * bb] = l < 0 ? -1 : (int)(compr[s2] + l);
+                    }
+            }
+            mcols.reset(P.n);
+            std::vector<int64_t> brow(nbatch);
+            std::vector<int64_t> bfull(nbatch);
+            for (size_t k = 0; k < batch.size(); ++k) {
+                const int64_t s2 = batch[k];
+                const int id = H.bsp[s2];
+                const int A = P.A[id], B = P.B[id], Na = b.nfunc[A], Nb = b.nfunc[B];
+                int* m = mcols.add(id, Na * Nb);
+                for (int bb = 0; bb < Nb; ++bb)
+                    for (int a = 0; a < Na; ++a) {
+                        const int64_t l = pair_local(a, bb, Na, A == B);
+                        m[a + Na * bb] = l < 0 ? -1 : (int)(colloc[k] + l);
+                    }
+                for (int i = 0; i < bdim(s2); ++i) {
+                    brow[colloc[k] + i] = compr[s2] + i;
+                    bfull[colloc[k] + i] = H.fullloc[s2] + i;
+                }
+            }
+            mrows.upload(s);
+            mcols.upload(s);
+            dM.ensure((size_t)ncand * nbatch);
+            std::vector<int> candids, batchids;
+            for (int64_t s2 : cand) candids.push_back(H.bsp[s2]);
+            for (int64_t s2 : batch) batchids.push_back(H.bsp[s2]);
+            T.start(kStep1Eri);
+            run_eri(H, candids, batchids, kModeProduct, &mrows, &mcols, dM.p, ncand);
+            T.stop();
+            // -------- chol2_SubtractR (:628-691): M -= L_cand L_batch^T
+            dbrow.upload(brow, s);
+            T.start(kSubtractR);
+            if (nchol > 0) {
+                dLB.ensure((size_t)nbatch * nchol);
+                CU(launch_gather_rows(Lst.p, ncand, dbrow.p, nbatch, nchol, dLB.p, nbatch, s));
+                gemm_nt(C.blas, ncand, nbatch, nchol, -1.0, Lst.p, ncand, dLB.p, nbatch, 1.0, dM.p, ncand);
+            }
+            T.stop();
+            // -------- micro iterations (:1025-1064) on the batch block
+            T.start(kPivots);
+            dMbb.ensure((size_t)nbatch * nbatch);
+            CU(launch_gather_rows(dM.p, ncand, dbrow.p, nbatch, nbatch, dMbb.p, nbatch, s));
+            dDb.ensure(nbatch);
+            CU(launch_gather_rows(dD.p, ncand, dbrow.p, nbatch, 1, dDb.p, nbatch, s));
+            dLb.ensure((size_t)nbatch * nbatch);
+            dpiv.ensure(nbatch);
+            dpdmax.ensure(nbatch);
+            CU(launch_pivot_batch(dMbb.p, (int)nbatch, dDb.p, dLb.p, dpiv.p, dpdmax.p, dnpiv.p, nchol, maxnchol, dmin, s));
+            int npiv = 0;
+            CU(cudaMemcpyAsync(&npiv, dnpiv.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CU(cudaStreamSynchronize(s));
+            std::vector<int> piv(npiv);
+            std::vector<double> pdm(npiv);
+            if (npiv > 0) {
+                CU(cudaMemcpyAsync(piv.data(), dpiv.p, sizeof(int) * npiv, cudaMemcpyDeviceToHost, s));
+                CU(cudaMemcpyAsync(pdm.data(), dpdmax.p, sizeof(double) * npiv, cudaMemcpyDeviceToHost, s));
+            }
+            if (npiv > 0) {
+                if (nchol + npiv > cap) {
+                    int64_t ncap = std::min<int64_t>(maxnchol, std::max<int64_t>(2 * cap, nchol + npiv));
+                    DVec<double> nL;
+                    nL.alloc((size_t)std::max<int64_t>(ncand, 1) * ncap);
+                    if (nchol > 0)
+                        CU(cudaMemcpyAsync(nL.p, Lst.p, sizeof(double) * ncand * nchol, cudaMemcpyDeviceToDevice, s));
+                    std::swap(Lst, nL);
+                    Lst2.release();
+                    cap = ncap;
+                }
+                // vectors over all candidates: L_new = M(:, piv) Lp^{-T}
+                dLp.ensure((size_t)npiv * npiv);
+                dLinv.ensure((size_t)npiv * npiv);
+                CU(launch_gather_pivrows(dLb.p, (int)nbatch, dpiv.p, npiv, dLp.p, s));
+                CU(launch_tri_inv_lower(dLp.p, npiv, dLinv.p, s));
+                dMp.ensure((size_t)ncand * npiv);
+                CU(launch_gather_cols(dM.p, ncand, dpiv.p, ncand, npiv, dMp.p, ncand, s));
+                gemm_nt(C.blas, ncand, npiv, npiv, 1.0, dMp.p, ncand, dLinv.p, npiv, 0.0, Lst.p + ncand * nchol, ncand);
+                CU(launch_downdate(dD.p, Lst.p + ncand * nchol, ncand, ncand, npiv, s));
+            }
+            T.stop();
+            CU(cudaStreamSynchronize(s));
+            for (int j = 0; j < npiv; ++j) {
+                const int64_t full = bfull[piv[j]];
+                H.pivots[full] = 1;
+                H.pivot_order.push_back(full);
+                H.pivot_dmax.push_back(pdm[j]);
+            }
+            nchol += npiv;
+        }
+        CU(launch_max(dD.p, ncand, dscal.p, s));
+        CU(cudaMemcpyAsync(&dmax, dscal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        T.flush();
+        if (ncand == 0) dmax = -1e300;
+        if (dmax <= H.tau) { converged = true; go = false; }
+        if (nchol == maxnchol || nbatch == 0) go = false;
+    }
+    H.nvecs = nchol;
+    H.nmacro = nmacro;
+    H.converged = converged ? 1 : 0;
+    if (nchol == maxnchol && !converged) fail(GCI_ERR_NOT_CONVERGED, "Max number of Cholesky vectors reached without convergence");
+}
+
+// ------------------------------------------------------------------ step 2
+static void pq2p_ge_q(int64_t pq, int64_t n, int64_t& p, int64_t& q)
+{   // chol2_pq2p_ge_q, TwoStepCholesky_Step2.f90:422-466 (1-based)
+    const int64_t q_base = (pq - 1) / (n + 1) + 1;
+    const int64_t v = pq - (n + 1) * (q_base - 1);
+    const int64_t interval1 = n - q_base + 1;
+    const int64_t in2 = v / (interval1 + 1);
+    const int64_t in1 = in2 ^ 1;
+    p = in1 * (q_base + v - 1) + in2 * (v - interval1 + n - q_base);
+    q = in1 * q_base + in2 * interval1;
+}
+
+static void step2(Handle& H)
+{
+    Context& C = ctx();
+    cudaStream_t s = C.stream;
+    const PairTable& P = H.pt;
+    const HostBasis& b = H.hb;
+    PhaseTimer& T = H.timer;
+    // chol2_PivotShellPairs (:469-534)
+    H.psp.clear(); H.psploc.clear(); H.pspdim.clear(); H.porb.clear();
+    int64_t q = 0;
+    for (int64_t s2 = 0; s2 < H.nsp; ++s2) {
+        const int id = H.bsp[s2];
+        const int A = P.A[id], B = P.B[id], Na = b.nfunc[A];
+        const int64_t p0 = H.fullloc[s2];
+        const int dim = P.dim[id];
+        int cnt = 0;
+        for (int i = 0; i < dim; ++i) cnt += H.pivots[p0 + i];
+        if (cnt == 0) continue;
+        H.psp.push_back((int)s2);
+        H.psploc.push_back(q);
+        H.pspdim.push_back(cnt);
+        for (int i = 0; i < dim; ++i) {
+            if (!H.pivots[p0 + i]) continue;
+            int full;
+            if (A != B) full = i;
+            else if (H.flags & GCI_FLAG_PIVOT_DECODE_STORAGE) {
+                int bb = 0, rem = i;
+                while (rem >= Na - bb) { rem -= Na - bb; ++bb; }
+                full = (bb + rem) + Na * bb;
+            } else {
+                int64_t pa, pb;
+                pq2p_ge_q(i + 1, Na, pa, pb);
+                full = (int)((pa - 1) + Na * (pb - 1));
+            }
+            H.porb.push_back(full);
+            ++q;
+        }
+    }
+    H.npsp = (int64_t)H.psp.size();
+    const int64_t N = H.nvecs;
+    if (q != N) fail(GCI_ERR_STATE, "Invalid Pivots array");
+    // pivot column map by pair id
+    H.pivmap.reset(P.n);
+    std::vector<int> pivids;
+    for (int64_t k = 0; k < H.npsp; ++k) {
+        const int id = H.bsp[H.psp[k]];
+        pivids.push_back(id);
+        int* m = H.pivmap.add(id, P.nab[id]);
+        for (int r = 0; r < H.pspdim[k]; ++r) m[H.porb[H.psploc[k] + r]] = (int)(H.psploc[k] + r);
+    }
+    H.pivmap.upload(s);
+    // chol2_Vpqrs (Step2.f90:76-187): here the full square (symmetric)
+    H.invl.alloc((size_t)std::max<int64_t>(N, 1) * std::max<int64_t>(N, 1));
+    if (N == 0) return;
+    CU(cudaMemsetAsync(H.invl.p, 0, sizeof(double) * N * N, s));
+    T.start(kVjjEri);
+    run_eri(H, pivids, pivids, kModeProduct, &H.pivmap, &H.pivmap, H.invl.p, N);
+    T.stop();
+    // real_Cholesky + real_LowerTriangularInverse (real_linalg.f90:39-72)
+    T.start(kPotrf);
+    int lwork = 0;
+    CS(cusolverDnDpotrf_bufferSize(C.solver, CUBLAS_FILL_MODE_LOWER, (int)N, H.invl.p, (int)N, &lwork));
+    DVec<double> work;
+    work.alloc(std::max(lwork, 1));
+    DVec<int> info;
+    info.alloc(1);
+    CS(cusolverDnDpotrf(C.solver, CUBLAS_FILL_MODE_LOWER, (int)N, H.invl.p, (int)N, work.p, lwork, info.p));
+    int hinfo = 0;
+    CU(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (hinfo != 0) fail(GCI_ERR_NOT_SPD, "dpotrf failed: info=" + std::to_string(hinfo));
+    CU(launch_zero_upper(H.invl.p, N, s));
+    size_t wdev = 0, whost = 0;
+    CS(cusolverDnXtrtri_bufferSize(C.solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, N, CUDA_R_64F, H.invl.p, N,
+                                   &wdev, &whost));
+    DVec<char> wd;
+    wd.alloc(std::max<size_t>(wdev, 1));
+    std::vector<char> wh(std::max<size_t>(whost, 1));
+    CS(cusolverDnXtrtri(C.solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, N, CUDA_R_64F, H.invl.p, N, wd.p, wdev,
+                        wh.data(), whost, info.p));
+    CU(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (hinfo != 0) fail(GCI_ERR_NOT_SPD, "dtrtri failed: info=" + std::to_string(hinfo));
+    T.stop();
+    T.flush();
+}
+
+// Full-dimension vectors, one subset at a time (TwoStepCholesky.f90:378-416)
+static void materialize_rkpq(Handle& H)
+{
+    Context& C = ctx();
+    cudaStream_t s = C.stream;
+    const PairTable& P = H.pt;
+    const HostBasis& b = H.hb;
+    const int64_t N = H.nvecs, msd = std::max<int64_t>(H.msd, 1);
+    H.rkpq.alloc((size_t)std::max<int64_t>(N, 1) * msd * H.nsubsets);
+    CU(cudaMemsetAsync(H.rkpq.p, 0, sizeof(double) * std::max<int64_t>(N, 1) * msd * H.nsubsets, s));
+    if (N == 0) { H.have_rkpq = true; return; }
+    DVec<double> W;
+    W.alloc((size_t)msd * N);
+    PairMap rows;
+    std::vector<int> pivids;
+    for (int64_t k = 0; k < H.npsp; ++k) pivids.push_back(H.bsp[H.psp[k]]);
+    for (int64_t X = 0; X < H.nsubsets; ++X) {
+        if (H.subsetlo[X] < 0) continue;
+        rows.reset(P.n);
+        std::vector<int> ids;
+        for (int64_t s2 = H.subsetlo[X]; s2 <= H.subsethi[X]; ++s2) {
+            const int id = H.bsp[s2];
+            ids.push_back(id);
+            const int A = P.A[id], B = P.B[id], Na = b.nfunc[A], Nb = b.nfunc[B];
+            int* m = rows.add(id, Na * Nb);
+            for (int bb = 0; bb < Nb; ++bb)
+                for (int a = 0; a < Na; ++a) {
+                    const int64_t l = pair_local(a, bb, Na, A == B);
+                    m[a + Na * bb] = l < 0 ? -1 : (int)(H.subloc[s2] + l);
+                }
+        }
+        rows.upload(s);
+        CU(cudaMemsetAsync(W.p, 0, sizeof(double) * msd * N, s));
+        H.timer.start(kFullEri);
+        run_eri(H, ids, pivids, kModeProduct, &rows, &H.pivmap, W.p, msd);
+        H.timer.stop();
+        // real_abT: Rkpq(:,:,X) = Inv_L W^T
+        H.timer.start(kInvLGemm);
+        gemm_nt(C.blas, N, msd, N, 1.0, H.invl.p, N, W.p, msd, 0.0, H.rkpq.p + (size_t)N * msd * X, N);
+        H.timer.stop();
+    }
+    CU(cudaStreamSynchronize(s));
+    H.timer.flush();
+    H.have_rkpq = true;
+}
+
+// ------------------------------------------------------------------ AO -> MO
+// GEMM1: W1[a][q][k] = sum_p CA[p][a] U[p][q][k]; GEMM2: out[b][a][k] = sum_q CB[q][b] W1[a][q][k]
+static void mo_two_gemms(Handle& H, int precision, const double* U, int64_t kc, const double* CAd, int64_t NA,
+                         const double* CBd, int64_t NB, double* W1, double* out, int64_t ldk)
+{
+    Context& C = ctx();
+    const int64_t nao = H.hb.nao;
+    const double one = 1.0, zero = 0.0;
+    if (precision == GCI_PREC_FP64) {
+        CB(cublasDgemm_64(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, nao * kc, NA, nao, &one, U, nao * kc, CAd, nao, &zero, W1,
+                          nao * kc));
+        CB(cublasDgemmStridedBatched_64(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, kc, NB, nao, &one, W1, kc, nao * kc, CBd,
+                                        nao, 0, &zero, out, ldk * NA, ldk, NA));
+    } else {
+        CU(mo_gemm_mixed(U, nao * kc, NA, nao, CAd, W1, C.stream));
+        CU(mo_gemm_mixed_batched(W1, kc, NB, nao, CBd, out, ldk, NA, C.stream));
+    }
+}
+
+static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int64_t a1, const double* CB_,
+                      int64_t ldcb, int64_t b0, int64_t b1, int64_t max_buffer_mb, int precision, double* rkab)
+{
+    Context& C = ctx();
+    cudaStream_t s = C.stream;
+    const PairTable& P = H.pt;
+    const HostBasis& b = H.hb;
+    const int64_t nao = b.nao, N = H.nvecs;
+    const int64_t NA = a1 - a0 + 1, NB = b1 - b0 + 1;
+    if (NA <= 0 || NB <= 0) fail(GCI_ERR_ARG, "Invalid dimension of Rkab");
+    if (ldca < nao || ldcb < nao) fail(GCI_ERR_ARG, "Invalid number of atomic orbitals in CA/CB");
+    if (precision != GCI_PREC_FP64 && precision != GCI_PREC_MIXED) fail(GCI_ERR_ARG, "invalid precision mode");
+    if (N == 0) return;
+    // MO coefficient blocks on the device
+    std::vector<double> ha((size_t)nao * NA), hbm((size_t)nao * NB);
+    for (int64_t a = 0; a < NA; ++a)
+        for (int64_t p = 0; p < nao; ++p) ha[p + nao * a] = CA[p + ldca * (a0 - 1 + a)];
+    for (int64_t a = 0; a < NB; ++a)
+        for (int64_t p = 0; p < nao; ++p) hbm[p + nao * a] = CB_[p + ldcb * (b0 - 1 + a)];
+    DVec<double> dCA, dCB, dOut, U, W1;
+    dCA.upload(ha, s);
+    dCB.upload(hbm, s);
+    dOut.alloc((size_t)N * NA * NB);
+    // chunk of the fastest index so that U + W1 fit in the buffer budget
+    const double budget = (max_buffer_mb > 0 ? (double)max_buffer_mb : 8192.0) * 1024.0 * 1024.0;
+    int64_t kc = (int64_t)(budget / (8.0 * (double)(nao * nao + nao * NA)));
+    if (kc < 1) fail(GCI_ERR_BUFFER, "Buffer size too small for Rpq->Rab");
+    kc = std::min<int64_t>(kc, N);
+    U.alloc((size_t)nao * nao * kc);
+    W1.alloc((size_t)nao * NA * kc);
+    PhaseTimer& T = H.timer;
+    if (H.have_rkpq) {
+        // reference order: from the stored Rkpq (Cholesky_Gammcor.f90:143-332)
+        std::vector<int64_t> pqcol;
+        std::vector<int> pqao;
+        for (int64_t s2 = 0; s2 < H.nsp; ++s2) {
+            const int id = H.bsp[s2];
+            const int A = P.A[id], B = P.B[id], Na = b.nfunc[A], Nb = b.nfunc[B];
+            const int64_t X = H.subidx[s2];
+            int64_t col = H.subloc[s2] + H.msd * X;
+            for (int bb = 0; bb < Nb; ++bb)
+                for (int a = (A == B) ? bb : 0; a < Na; ++a) {
+                    pqcol.push_back(col++);
+                    pqao.push_back(b.loc[A] + a);
+                    pqao.push_back(b.loc[B] + bb);
+                }
+        }
+        DVec<int64_t> dcol;
+        DVec<int> dao;
+        dcol.upload(pqcol, s);
+        dao.upload(pqao, s);
+        for (int64_t k0 = 0; k0 < N; k0 += kc) {
+            const int64_t kk = std::min(kc, N - k0);
+            T.start(kMoGemm);
+            CU(cudaMemsetAsync(U.p, 0, sizeof(double) * nao * nao * kk, s));
+            CU(launch_unpack_rkpq(H.rkpq.p, N, dcol.p, dao.p, (int64_t)pqcol.size(), k0, kk, nao, U.p, s));
+            mo_two_gemms(H, precision, U.p, kk, dCA.p, NA, dCB.p, NB, W1.p, dOut.p + k0, N);
+            T.stop();
+        }
+    } else {
+        // direct: V(pq, J) chunks -> Vab(J, a, b) -> Rkab = Inv_L Vab
+        DVec<double> Vab;
+        Vab.alloc((size_t)N * NA * NB);
+        std::vector<int> baseids;
+        for (int64_t s2 = 0; s2 < H.nsp; ++s2) baseids.push_back(H.bsp[s2]);
+        int64_t k = 0;
+        while (k < H.npsp) {
+            const int64_t J0 = H.psploc[k];
+            int64_t k1 = k;
+            while (k1 < H.npsp && H.psploc[k1] + H.pspdim[k1] - J0 <= kc) ++k1;
+            if (k1 == k) ++k1;   // one pivot pair always fits (kc >= 1 pair of at most 49 columns)
+            const int64_t J1 = H.psploc[k1 - 1] + H.pspdim[k1 - 1];
+            const int64_t jc = J1 - J0;
+            if (jc > kc) fail(GCI_ERR_BUFFER, "Buffer size too small for Rpq->Rab");
+            PairMap cm;
+            cm.reset(P.n);
+            std::vector<int> kids;
+            for (int64_t q = k; q < k1; ++q) {
+                const int id = H.bsp[H.psp[q]];
+                kids.push_back(id);
+                int* m = cm.add(id, P.nab[id]);
+                for (int r = 0; r < H.pspdim[q]; ++r) m[H.porb[H.psploc[q] + r]] = (int)(H.psploc[q] + r - J0);
+            }
+            cm.upload(s);
+            CU(cudaMemsetAsync(U.p, 0, sizeof(double) * nao * nao * jc, s));
+            T.start(kFullEri);
+            run_eri(H, baseids, kids, kModeDense, nullptr, &cm, U.p, 0, jc);
+            T.stop();
+            T.start(kMoGemm);
+            mo_two_gemms(H, precision, U.p, jc, dCA.p, NA, dCB.p, NB, W1.p, Vab.p + J0, N);
+            T.stop();
+            CU(cudaStreamSynchronize(s));
+            k = k1;
+        }
+        T.start(kInvLGemm);
+        const double one = 1.0, zero = 0.0;
+        CB(cublasDgemm_64(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, NA * NB, N, &one, H.invl.p, N, Vab.p, N, &zero, dOut.p, N));
+        T.stop();
+    }
+    CU(cudaMemcpyAsync(rkab, dOut.p, sizeof(double) * N * NA * NB, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    T.flush();
+}
+
+} // namespace gci
+
+// =================================================================== C ABI
+using namespace gci;
+
+struct gci_handle {
+    Handle h;
+};
+
+extern "C" {
+
+int gci_init(void)
+{
+    return guarded([&] { ctx(); });
+}
+
+int gci_rkpq(const gci_basis* basis, int accuracy, double omega, int flags, gci_handle** out)
+{
+    if (!out) { g_last_error = "out is NULL"; return GCI_ERR_ARG; }
+    *out = nullptr;
+    std::unique_ptr<gci_handle> hp(new gci_handle());
+    const int rc = guarded([&] {
+        Handle& H = hp->h;
+        H.tau = accuracy_tau(accuracy);
+        H.kappa = (omega > 0.0) ? 1.0 / (omega * omega) : 0.0;   // Cholesky_Gammcor.f90:412-421
+        H.flags = flags;
+        Context& C = ctx();
+        H.timer.s = C.stream;
+        auto t0 = std::chrono::steady_clock::now();
+        H.hb = make_basis(basis);
+        setup_pairs(H);
+        step1(H);
+        step2(H);
+        if (flags & GCI_FLAG_MATERIALIZE_RKPQ) materialize_rkpq(H);
+        CU(cudaStreamSynchronize(C.stream));
+        H.t_rkpq = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    });
+    if (rc == GCI_OK) *out = hp.release();
+    return rc;
+}
+
+int gci_query(const gci_handle* h, int64_t* nvecs, int64_t* max_subset_dim, int64_t* nsubsets, int64_t* norbpairs,
+              int64_t* nshellpairs, int64_t* npivshellpairs)
+{
+    if (!h) { g_last_error = "handle is NULL"; return GCI_ERR_ARG; }
+    const Handle& H = h->h;
+    if (nvecs) *nvecs = H.nvecs;
+    if (max_subset_dim) *max_subset_dim = H.msd;
+    if (nsubsets) *nsubsets = H.nsubsets;
+    if (norbpairs) *norbpairs = H.npq;
+    if (nshellpairs) *nshellpairs = H.nsp;
+    if (npivshellpairs) *npivshellpairs = H.npsp;
+    return GCI_OK;
+}
+
+int gci_copy_rkpq(const gci_handle* h, double* dst)
+{
+    if (!h || !dst) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        const Handle& H = h->h;
+        if (!H.have_rkpq) fail(GCI_ERR_STATE, "Rkpq was not materialised (pass GCI_FLAG_MATERIALIZE_RKPQ)");
+        const size_t n = (size_t)H.nvecs * H.msd * H.nsubsets;
+        if (n) CU(cudaMemcpy(dst, H.rkpq.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+int gci_copy_chol2data(const gci_handle* h, int64_t* shellpairs, int64_t* shellpairloc, int64_t* shellpairdim,
+                       int64_t* subsetdim, int64_t* subsetbounds, int64_t* pivots, int64_t* pivotshellpairs,
+                       int64_t* pivotshellpairloc, int64_t* pivotshellpairdim, int64_t* pivotorbpairs, double* inv_l)
+{
+    if (!h) { g_last_error = "handle is NULL"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        const Handle& H = h->h;
+        const PairTable& P = H.pt;
+        for (int64_t s2 = 0; s2 < H.nsp; ++s2) {
+            const int id = H.bsp[s2];
+            if (shellpairs) { shellpairs[2 * s2] = P.A[id] + 1; shellpairs[2 * s2 + 1] = P.B[id] + 1; }
+            if (shellpairloc) {
+                shellpairloc[3 * s2] = H.fullloc[s2] + 1;
+                shellpairloc[3 * s2 + 1] = H.subloc[s2] + 1;
+                shellpairloc[3 * s2 + 2] = H.subidx[s2] + 1;
+            }
+            if (shellpairdim) shellpairdim[s2] = P.dim[id];
+        }
+        for (int64_t X = 0; X < H.nsubsets; ++X) {
+            if (subsetdim) subsetdim[X] = H.subsetdim[X];
+            if (subsetbounds) { subsetbounds[2 * X] = H.subsetlo[X] + 1; subsetbounds[2 * X + 1] = H.subsethi[X] + 1; }
+        }
+        if (pivots) for (int64_t p = 0; p < H.npq; ++p) pivots[p] = H.pivots[p];
+        for (int64_t k = 0; k < H.npsp; ++k) {
+            if (pivotshellpairs) pivotshellpairs[k] = H.psp[k] + 1;
+            if (pivotshellpairloc) pivotshellpairloc[k] = H.psploc[k] + 1;
+            if (pivotshellpairdim) pivotshellpairdim[k] = H.pspdim[k];
+        }
+        if (pivotorbpairs) for (int64_t q = 0; q < H.nvecs; ++q) pivotorbpairs[q] = H.porb[q] + 1;
+        if (inv_l && H.nvecs > 0)
+            CU(cudaMemcpy(inv_l, H.invl.p, sizeof(double) * H.nvecs * H.nvecs, cudaMemcpyDeviceToHost));
+    });
+}
+
+int gci_pivot_order(const gci_handle* h, int64_t* order, double* dmax)
+{
+    if (!h) { g_last_error = "handle is NULL"; return GCI_ERR_ARG; }
+    const Handle& H = h->h;
+    for (size_t j = 0; j < H.pivot_order.size(); ++j) {
+        if (order) order[j] = H.pivot_order[j] + 1;
+        if (dmax) dmax[j] = H.pivot_dmax[j];
+    }
+    return GCI_OK;
+}
+
+int gci_rkab(gci_handle* h, const double* CA, int64_t ldca, int64_t a0, int64_t a1, const double* CB,
+             int64_t ldcb, int64_t b0, int64_t b1, int64_t max_buffer_mb, int precision, double* rkab)
+{
+    if (!h || !CA || !CB || !rkab) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        auto t0 = std::chrono::steady_clock::now();
+        rkab_impl(h->h, CA, ldca, a0, a1, CB, ldcb, b0, b1, max_buffer_mb, precision, rkab);
+        h->h.t_rkab = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    });
+}
+
+int gci_timings(const gci_handle* h, double* out, int n)
+{
+    if (!h || !out) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    const Handle& H = h->h;
+    double v[13];
+    for (int i = 0; i < kNumPhases; ++i) v[i] = H.timer.acc[i];
+    v[10] = (double)H.nmacro;
+    v[11] = H.t_rkpq;
+    v[12] = H.t_rkab;
+    for (int i = 0; i < n && i < 13; ++i) out[i] = v[i];
+    return GCI_OK;
+}
+
+void gci_free(gci_handle* h) { delete h; }
+
+const char* gci_last_error(void) { return g_last_error.c_str(); }
+
+int gci_boys(int m, int64_t n, const double* x, double* out)
+{
+    if (m < 0 || m > kBoysMaxM || n < 0 || (n > 0 && (!x || !out))) { g_last_error = "invalid argument"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        Context& C = ctx();
+        DVec<double> dx, dout;
+        std::vector<double> hx(x, x + n);
+        dx.upload(hx, C.stream);
+        dout.alloc((size_t)std::max<int64_t>(n, 1) * (m + 1));
+        CU(boys_eval_launch(m, n, dx.p, C.boys.p, dout.p, C.stream));
+        if (n) CU(cudaMemcpyAsync(out, dout.p, sizeof(double) * n * (m + 1), cudaMemcpyDeviceToHost, C.stream));
+        CU(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int gci_spher_coeffs(int L, double* U)
+{
+    if (L < 0 || L > 6 || !U) { g_last_error = "invalid argument"; return GCI_ERR_ARG; }
+    spher_coeffs(L, U);
+    return GCI_OK;
+}
+
+int gci_normalize_basis(int64_t nparams, int64_t ldprim, const int64_t* L, const int64_t* nprim, const double* exps,
+                        double* coefs, double* norm_cart, int64_t ldcart, double* norm_spher, int64_t ldsph)
+{
+    if (nparams < 0 || !L || !nprim || !exps || !coefs) { g_last_error = "invalid argument"; return GCI_ERR_ARG; }
+    for (int64_t a = 0; a < nparams; ++a) {
+        if (L[a] < 0 || L[a] > 6 || nprim[a] < 1 || nprim[a] > ldprim) { g_last_error = "invalid shell"; return GCI_ERR_ARG; }
+        if ((norm_cart && ldcart < ncart((int)L[a])) || (norm_spher && ldsph < 2 * L[a] + 1)) {
+            g_last_error = "norm leading dimension too small";
+            return GCI_ERR_ARG;
+        }
+    }
+    normalize_basis(nparams, ldprim, L, nprim, exps, coefs, norm_cart, ldcart, norm_spher, ldsph);
+    return GCI_OK;
+}
+
+int gci_eri_pairs(const gci_basis* basis, double omega, double* out, int64_t ld)
+{
+    if (!out) { g_last_error = "out is NULL"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        Context& C = ctx();
+        Handle H;
+        H.timer.s = C.stream;
+        H.kappa = (omega > 0.0) ? 1.0 / (omega * omega) : 0.0;
+        H.hb = make_basis(basis);
+        setup_pairs(H);
+        const PairTable& P = H.pt;
+        int64_t npq = 0;
+        for (int64_t i = 0; i < P.n; ++i) npq += P.dim[i];
+        if (ld < npq) fail(GCI_ERR_ARG, "leading dimension too small");
+        PairMap m;
+        m.reset(P.n);
+        std::vector<int> all(P.n);
+        for (int64_t sp = 0; sp < P.n; ++sp) {
+            all[sp] = (int)sp;
+            const int A = P.A[sp], B = P.B[sp], Na = H.hb.nfunc[A], Nb = H.hb.nfunc[B];
+            int* mm = m.add((int)sp, Na * Nb);
+            for (int bb = 0; bb < Nb; ++bb)
+                for (int a = 0; a < Na; ++a) {
+                    const int64_t l = pair_local(a, bb, Na, A == B);
+                    mm[a + Na * bb] = l < 0 ? -1 : (int)(P.vdloc[sp] + l);
+                }
+        }
+        m.upload(C.stream);
+        DVec<double> d;
+        d.alloc((size_t)ld * npq);
+        CU(cudaMemsetAsync(d.p, 0, sizeof(double) * ld * npq, C.stream));
+        run_eri(H, all, all, kModeProduct, &m, &m, d.p, ld);
+        CU(cudaMemcpyAsync(out, d.p, sizeof(double) * ld * npq, cudaMemcpyDeviceToHost, C.stream));
+        CU(cudaStreamSynchronize(C.stream));
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,88 @@
+// gci_common.h -- definitions shared by the host runtime and the sm_100a kernels
+// of the integral-direct Cholesky ERI library.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define GCI_HD __host__ __device__ __forceinline__
+
+namespace gci {
+
+// Highest angular momentum handled by the GPU ERI kernels (f shells).  The
+// reference engine goes to h (auto2e.f90:275); classes above f are rejected
+// with an error by the host runtime.
+constexpr int kMaxL = 3;
+constexpr int kMaxPairL = 2 * kMaxL;          // bra or ket level
+constexpr int kMaxLT = 2 * kMaxPairL;         // total Hermite level
+constexpr int kMaxDerivLT = kMaxLT + 1;       // adjoint kernels shift one level up
+constexpr int kBoysMaxM = 20;                 // table order, 4*AUTO2E_MAXL (Cholesky_Gammcor.f90:350)
+constexpr int kBoysNInt = 500;                // intervals on [0, 25)  (boys.f90:20-21,43)
+constexpr double kBoysXAsym = 25.0;
+constexpr double kBoysDelta = kBoysXAsym / kBoysNInt;
+constexpr double kPi = 3.14159265358979323846264338327950288;
+
+GCI_HD constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+GCI_HD constexpr int cart_off(int l) { return l * (l + 1) * (l + 2) / 6; }
+GCI_HD constexpr int herm_n(int n) { return (n + 1) * (n + 2) * (n + 3) / 6; }
+GCI_HD constexpr int tri(int l) { return (l + 1) * (l + 2) / 2; }
+// Hermite index, level-major: all (t,u,v) with t+u+v < n precede level n.
+GCI_HD constexpr int herm_idx(int t, int u, int v)
+{
+    return (t + u + v) * (t + u + v + 1) * (t + u + v + 2) / 6 + (u + v) * (u + v + 1) / 2 + v;
+}
+// Position of (lx,ly,lz) within its level, Auto2e order (lx desc, ly desc).
+GCI_HD constexpr int cart_pos(int ly, int lz) { return (ly + lz) * (ly + lz + 1) / 2 + lz; }
+// Shell pair type for l_hi >= l_lo: 0..9 for l <= 3.
+GCI_HD constexpr int pair_type(int lhi, int llo) { return lhi * (lhi + 1) / 2 + llo; }
+constexpr int kNumPairTypes = pair_type(kMaxL, kMaxL) + 1;
+
+// Size in doubles of one primitive-pair record of a pair whose level is L1:
+//   [0] P  [1..3] Rp  [4] K_ab c_a c_b  [5..7] Rp - A  [8..] E^{e}_t, x/y/z
+GCI_HD constexpr int pp_record(int l1) { return 8 + 3 * tri(l1); }
+
+// Output modes of the ERI kernels.
+enum EriMode : int {
+    kModeProduct = 0,    // every (bra, ket) combination, written through row/col maps
+    kModeDiagonal = 1,   // bra == ket, only (ab|ab) kept: out[rowmap(ab)]
+    kModeDense = 2,      // bra pair x ket pair into a dense AO-pair layout (both triangles)
+};
+
+struct ShellPairDev {
+    int s1, s2;          // canonical shells: s1 has the higher (or equal) L
+    int swap;            // 1 if s1 is the second shell of the stored pair (A >= B index order)
+    int nprim1, nprim2;
+    int l1, l2;          // angular momenta of s1, s2
+    int64_t rec_off;     // offset (doubles) of the first primitive-pair record
+};
+
+struct EriArgs {
+    // basis
+    const double* sh_xyz;     // 3 per shell
+    const int* sh_toff;       // offset of the shell's transform in tmat
+    const double* tmat;       // per shell nfunc x ncart, row-major
+    const int* sh_nfunc;
+    const int* sh_loc;        // first AO index of each shell (dense mode)
+    // pairs
+    const ShellPairDev* pairs;
+    const double* pp;         // primitive-pair records
+    // task space: bra list x ket list (actual orientation)
+    const int* bra_ids;
+    const int* ket_ids;
+    int64_t nbra, nket;
+    int swap_bk;              // 1: the canonical bra is the actual ket pair
+    int mode;
+    // output
+    double* out;
+    int64_t ldo;
+    const int64_t* row_off;   // per pair id: offset into row_map (entries Na*Nb)
+    const int* row_map;
+    const int64_t* col_off;
+    const int* col_map;
+    int64_t nao;              // dense mode: AO count; out is [p][q][j] with j fastest
+    int64_t jcount;           // dense mode: extent of the fastest index
+    double kappa;
+    const double* boys;       // (kBoysMaxM+1) x kBoysNInt x 5
+    int* err;                 // device error word
+};
+
+} // namespace gci

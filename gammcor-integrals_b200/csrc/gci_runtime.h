@@ -1,0 +1,28 @@
+// gci_runtime.h -- host-side declarations of the kernel launchers.
+#pragma once
+#include "gci_common.h"
+
+namespace gci {
+
+cudaError_t eri_module_init();
+cudaError_t eri_launch(int tb, int tk, const EriArgs& args, cudaStream_t st);
+cudaError_t pair_records_launch(const ShellPairDev* pairs, int npairs, const double* xyz, const int* poff,
+                                const double* exps, const double* coefs, double* pp, cudaStream_t st);
+cudaError_t boys_eval_launch(int m, int64_t n, const double* x, const double* table, double* out, cudaStream_t st);
+
+cudaError_t launch_segmax(const double* D, const int64_t* loc, const int* dim, int64_t n, double* out, cudaStream_t s);
+cudaError_t launch_gather_rows(const double* src, int64_t lds, const int64_t* idx, int64_t nrows, int64_t ncols,
+                               double* dst, int64_t ldd, cudaStream_t s);
+cudaError_t launch_gather_cols(const double* src, int64_t lds, const int* cols, int64_t nrows, int64_t ncols,
+                               double* dst, int64_t ldd, cudaStream_t s);
+cudaError_t launch_pivot_batch(const double* Mbb, int nb, double* Db, double* Lb, int* piv, double* pdmax,
+                               int* npiv, int64_t nchol0, int64_t maxnchol, double dmin, cudaStream_t s);
+cudaError_t launch_gather_pivrows(const double* Lb, int nb, const int* piv, int npiv, double* Lp, cudaStream_t s);
+cudaError_t launch_tri_inv_lower(const double* L, int n, double* X, cudaStream_t s);
+cudaError_t launch_downdate(double* D, const double* L, int64_t ld, int64_t n, int ncols, cudaStream_t s);
+cudaError_t launch_max(const double* v, int64_t n, double* out, cudaStream_t s);
+cudaError_t launch_zero_upper(double* A, int64_t n, cudaStream_t s);
+cudaError_t launch_unpack_rkpq(const double* R, int64_t nvecs, const int64_t* pq_col, const int* pq_ao, int64_t npq,
+                               int64_t k0, int64_t kc, int64_t nao, double* U, cudaStream_t s);
+
+} // namespace gci

@@ -1,0 +1,146 @@
+/*
+ * gci.h -- C ABI of the B200 integral-direct Cholesky ERI library
+ * (libgci.so).  Plain pointers and sizes only; every call returns an int
+ * status (0 = success, negative = error) and gci_last_error() gives the
+ * message of the last failure on the calling thread.
+ *
+ * This is the drop-in boundary for the reference's Gammcor interface
+ * (modrzejewski/gammcor-integrals, src/gammcor-interface/Cholesky_Gammcor.f90).
+ * A Fortran ISO_C_BINDING shim keeping the module Cholesky_Gammcor and the
+ * type TCholeskyVecsOTF binds these entry points.
+ *
+ * Conventions: arrays are column-major (Fortran order); indices passed in
+ * arrays are 1-based exactly as in TAOBasis; integers are int64_t so that
+ * both default-integer and -i8 builds of the caller can convert losslessly.
+ */
+#ifndef GCI_H
+#define GCI_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define GCI_OK                 0
+#define GCI_ERR_ARG           -1   /* invalid argument / dimension       */
+#define GCI_ERR_CUDA          -2   /* CUDA, cuBLAS or cuSOLVER failure    */
+#define GCI_ERR_UNSUPPORTED   -3   /* angular momentum beyond the kernels */
+#define GCI_ERR_NOT_CONVERGED -4   /* MaxNCholesky reached unconverged    */
+#define GCI_ERR_NOT_SPD       -5   /* pivot block V_JJ not positive definite */
+#define GCI_ERR_BUFFER        -6   /* buffer too small                    */
+#define GCI_ERR_NOMEM         -7   /* device allocation failed            */
+#define GCI_ERR_STATE         -8   /* handle lacks the requested data     */
+
+/* Accuracy levels: CHOL_ACCURACY_* of Cholesky_Gammcor.f90:14-17 */
+#define GCI_ACCURACY_DEFAULT   1   /* tau = 1e-5  */
+#define GCI_ACCURACY_TIGHT     2   /* tau = 1e-6  */
+#define GCI_ACCURACY_LUDICROUS 3   /* tau = 1e-7  */
+#define GCI_ACCURACY_DEBUG     4   /* tau = 1e-10 */
+
+/* gci_rkpq flags */
+#define GCI_FLAG_MATERIALIZE_RKPQ   1  /* store Rkpq on the device (otherwise Rkab is built from V(pq,J) directly) */
+#define GCI_FLAG_PIVOT_DECODE_STORAGE 2 /* decode diagonal-shell-pair pivots in storage order (the reference decodes
+                                          them with chol2_pq2p_ge_q, TwoStepCholesky_Step2.f90:422-466) */
+#define GCI_FLAG_MIXED_STEP1        4  /* split-precision tensor-core GEMMs in the pivot search */
+
+/* Precision of the AO->MO GEMMs */
+#define GCI_PREC_FP64   0
+#define GCI_PREC_MIXED  1
+
+/* Orbital orderings: ORBITAL_ORDERING_* of Auto2eInterface.f90:12-17 */
+#define GCI_ORDERING_AUTO2E      0
+#define GCI_ORDERING_MOLPRO      1
+#define GCI_ORDERING_ORCA        2
+#define GCI_ORDERING_DALTON      3
+#define GCI_ORDERING_OPEN_MOLCAS 4
+#define GCI_ORDERING_PYSCF       5
+
+/* The arrays of TAOBasis (basis_definitions.f90:94-192) the path reads. */
+typedef struct {
+    int64_t natoms, nshells, nshellparams;
+    int64_t ldprim;                  /* leading dim of cntr_coeffs/exponents (MaxNPrimitives) */
+    int64_t ldnorm;                  /* leading dim of norm_factors */
+    const double *atom_coords;       /* AtomCoords(3, NAtoms) */
+    const int64_t *shell_centers;    /* ShellCenters(NShells), 1-based atom */
+    const int64_t *shell_params_idx; /* ShellParamsIdx(NShells), 1-based */
+    const int64_t *shell_momentum;   /* ShellMomentum(NShellParams) */
+    const int64_t *nprimitives;      /* NPrimitives(NShellParams) */
+    const double *cntr_coeffs;       /* CntrCoeffs(ldprim, NShellParams), primitive norms folded in */
+    const double *exponents;         /* Exponents(ldprim, NShellParams) */
+    const double *norm_factors;      /* NormFactorsSpher or NormFactorsCart(ldnorm, NShellParams) */
+    int32_t spher_ao;                /* SpherAO */
+} gci_basis;
+
+typedef struct gci_handle gci_handle;
+
+/* Library/device initialisation (auto2e_init + boys_init, Cholesky_Gammcor.f90:347-350).
+ * Idempotent. */
+int gci_init(void);
+
+/* chol_gammcor_Rkpq (Cholesky_Gammcor.f90:335-377) + chol_gammcor_CoulombMatrix (:380-441):
+ * two-step Cholesky (chol2_Algo_Koch_JCP2019, TwoStepCholesky.f90:45-71).  omega <= 0 means
+ * the full-range Coulomb operator (Kappa = 0). */
+int gci_rkpq(const gci_basis *basis, int accuracy, double omega, int flags, gci_handle **out);
+
+/* Dimensions of TCholeskyVecsOTF / TChol2Vecs (TwoStepCholesky_definitions.f90:56-74). */
+int gci_query(const gci_handle *h, int64_t *nvecs, int64_t *max_subset_dim, int64_t *nsubsets,
+              int64_t *norbpairs, int64_t *nshellpairs, int64_t *npivshellpairs);
+
+/* Rkpq(NVecs, MaxSubsetDim, NSubsets) -> host, column-major (TCholeskyVecsOTF%Rkpq). */
+int gci_copy_rkpq(const gci_handle *h, double *dst);
+
+/* Chol2Data arrays (TChol2Vecs), 1-based indices as the Fortran type holds them.
+ * Any pointer may be NULL.  Sizes: shellpairs 2 x NShellPairs, shellpairloc 3 x NShellPairs,
+ * shellpairdim NShellPairs, subsetdim/subsetbounds(2x) NSubsets, pivots NOrbPairs,
+ * pivotshellpairs/loc/dim NPivotShellPairs, pivotorbpairs NVecs, inv_l NVecs x NVecs. */
+int gci_copy_chol2data(const gci_handle *h, int64_t *shellpairs, int64_t *shellpairloc, int64_t *shellpairdim,
+                       int64_t *subsetdim, int64_t *subsetbounds, int64_t *pivots, int64_t *pivotshellpairs,
+                       int64_t *pivotshellpairloc, int64_t *pivotshellpairdim, int64_t *pivotorbpairs,
+                       double *inv_l);
+
+/* Pivot sequence of step 1 (FULL-storage orbital-pair indices, 1-based, selection order)
+ * and the residual diagonal at each selection.  Either pointer may be NULL. */
+int gci_pivot_order(const gci_handle *h, int64_t *order, double *dmax);
+
+/* chol_gammcor_Rkab (Cholesky_Gammcor.f90:26-92) after the AO-order conversion done by
+ * the caller (auto2e_interface_AngFuncTransf): CA(ldca, *), CB(ldcb, *) in Auto2e AO order,
+ * columns a0..a1 and b0..b1 (1-based inclusive).  Rkab(NVecs, NA*NB), k fastest, then a,
+ * then b.  max_buffer_mb bounds the AO->MO work buffers (MaxBufferDimMB). */
+int gci_rkab(gci_handle *h, const double *CA, int64_t ldca, int64_t a0, int64_t a1,
+             const double *CB, int64_t ldcb, int64_t b0, int64_t b1, int64_t max_buffer_mb,
+             int precision, double *rkab);
+
+/* Per-phase device times (seconds) of the last gci_rkpq/gci_rkab on this handle:
+ * [0] Vdiag [1] step-1 ERI (time_2e) [2] M - L L^T (time_rTr) [3] pivots + vectors (time_rk)
+ * [4] compress [5] V_JJ ERI [6] potrf+trtri [7] full-dim ERI [8] Inv_L GEMM [9] AO->MO GEMMs
+ * [10] step-1 macro iterations (count) [11] total rkpq wall [12] total rkab wall. */
+int gci_timings(const gci_handle *h, double *out, int n);
+
+void gci_free(gci_handle *h);
+const char *gci_last_error(void);
+
+/* ---- kernel-level entry points (no reference counterpart beyond the cited routine) ---- */
+
+/* Boys function on the device: out[i*(m+1)+k] = F_k(x[i]), k = 0..m (fm, boys.f90:224-281). */
+int gci_boys(int m, int64_t n, const double *x, double *out);
+
+/* Real-solid-harmonic coefficients, (2L+1) x ncart(L) row-major, m = -L..L
+ * (AutoSpherTransf.py:147-160 as used by auto2e_SpherTransf.f90). Host only. */
+int gci_spher_coeffs(int L, double *U);
+
+/* basis_NormalizeCntrCoeffs (basis_sets.f90:894-945) in place + SpherGTO_NormFactors
+ * (sphergto.f90:166-211).  Host only. */
+int gci_normalize_basis(int64_t nparams, int64_t ldprim, const int64_t *L, const int64_t *nprim,
+                        const double *exps, double *coefs, double *norm_cart, int64_t ldcart,
+                        double *norm_spher, int64_t ldsph);
+
+/* Every shell-pair x shell-pair ERI block (pq|rs) of a basis: out is NPQ x NPQ, column-major,
+ * with orbital pairs in the chol2_Vdiag order (ShB outer, ShA >= ShB inner; a fastest, lower
+ * triangle for ShA == ShB).  Small bases only (tests). */
+int gci_eri_pairs(const gci_basis *basis, double omega, double *out, int64_t ld);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
