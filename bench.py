@@ -1,0 +1,342 @@
+#!/usr/bin/env python3
+"""Benchmark of the integral-direct Cholesky ERI + AO->MO path on B200.
+
+One step = one complete job on a seeded synthetic molecule: the two-step
+Cholesky decomposition of (pq|rs) (diagonal, pivot search, pivot block,
+Inv_L) and the AO->MO transformation of the Cholesky vectors into the
+occupied x virtual block, through the library's C ABI (libgci.so).
+
+``value`` is the algorithmic GFLOP/s of the job (flops.py: GEMM formulas +
+per-class ERI arithmetic) with the inputs resident on the device, timed with
+CUDA events on the library's stream; ``e2e`` is the same job through the
+host API (TAOBasis + MO coefficients in pinned host memory, Rkab read back).
+``--impl reference`` times the CPU restatement of the reference algorithm
+(oracle/, all host threads) on a bounded sample of the same workload.
+
+Multi-GPU: the path runs as independent replicas (one job per rank); value is
+the flops of all ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Cholesky-ERI wall time & GFLOP/s, mixed vs FP64 on B200 at ≤1e-8 max ERI err"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--buffer-mb", type=int, default=16384)
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_fp64_peak(torch):
+    """FP64 reference rate for the roofline (MEASURED_PEAKS.json has no FP64
+    figure): cuBLAS DGEMM 8192^3, best of 5, CUDA events."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_baseline_c1():
+    """The oracle (FP64 C restatement, all host threads) on the full c1 job."""
+    from gammcor_integrals_b200 import flops, molecules
+    from oracle import oracle as O
+    m = molecules.config("c1")
+    b = O.make_basis(m.atoms, m.shells)
+    O.stats_reset()
+    t0 = time.perf_counter()
+    ch = O.cholesky(b, m.tau)
+    nocc, nvirt, seed = molecules.MO_SPLIT["c1"]
+    Cm = molecules.mo_coefficients(b.nao, seed)
+    O.mo_transf(ch, b, Cm, 0, nocc - 1, Cm, nocc, nocc + nvirt - 1)
+    dt = time.perf_counter() - t0
+    O.free(ch)
+    f = flops.job_flops(O.stats(), 21)
+    return {"value": f["total"] / dt / 1e9, "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"full c1 job (10 atoms, NAO={b.nao}, {ch.nvecs} vectors, MO 20x60) in {dt:.1f} s "
+                      f"on the oracle (FP64 C restatement of the reference, OpenMP)",
+            "seconds": dt}
+
+
+def run_reference(args, rank):
+    """--impl reference: the oracle on a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    from gammcor_integrals_b200 import flops, molecules
+    from oracle import oracle as O
+    m = molecules.config(args.config)
+    b = O.make_basis(m.atoms, m.shells)
+    sample = "c1 full job" if args.config != "c1" else "c1 full job"
+    # c2 and larger: one step = the full c1 job (the diagonal stage of c2 alone takes > 1 min on 8 cores)
+    mol = molecules.config("c1")
+    ob = O.make_basis(mol.atoms, mol.shells)
+    nocc, nvirt, seed = molecules.MO_SPLIT["c1"]
+    Cm = molecules.mo_coefficients(ob.nao, seed)
+
+    def step():
+        O.stats_reset()
+        t0 = time.perf_counter()
+        ch = O.cholesky(ob, mol.tau)
+        O.mo_transf(ch, ob, Cm, 0, nocc - 1, Cm, nocc, nocc + nvirt - 1)
+        dt = time.perf_counter() - t0
+        O.free(ch)
+        return dt, flops.job_flops(O.stats(), 21)["total"]
+
+    for _ in range(max(0, min(args.warmup, 1))):
+        step()
+    tt, ff = 0.0, 0.0
+    for _ in range(args.steps):
+        dt, f = step()
+        tt += dt
+        ff += f
+    v = ff / tt / 1e9
+    cores = os.cpu_count()
+    line = {"metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"{sample} (10 atoms, NAO={ob.nao}), bounded sample of {args.config}",
+                       "tau": mol.tau},
+            "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+                             "sample": f"{sample}: oracle (FP64 C restatement, OpenMP {cores} threads); "
+                                       f"the Fortran reference cannot be compiled here"},
+            "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=torch.device("cuda", local))
+    import gammcor_pkg
+    gammcor_pkg.load()
+    from gammcor_integrals_b200 import _capi, basis, flops, molecules
+    from gammcor_integrals_b200 import cholesky_gammcor as cg
+    L = _capi.lib()
+    _capi.check(L.gci_init())
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    mol = molecules.config(args.config)
+    tb = basis.from_molecule(mol)
+    nao = tb.NAO
+    nocc, nvirt, seed = molecules.MO_SPLIT.get(args.config, (20, 60, 101))
+    Cm = molecules.mo_coefficients(nao, seed)
+    a0, a1, b0, b1 = 1, nocc, nocc + 1, nocc + nvirt
+    NA, NB = nocc, nvirt
+    prec = {"fp64": _capi.GCI_PREC_FP64, "mixed": _capi.GCI_PREC_MIXED}[args.precision]
+    c_dev = torch.from_numpy(np.ascontiguousarray(Cm.T)).cuda()    # column-major C on the device
+    sptr = C.c_void_p()
+    _capi.check(L.gci_get_stream(C.byref(sptr)))
+    lib_stream = torch.cuda.ExternalStream(sptr.value)
+    bstruct = tb.c_struct()
+    state = {"rkab": None, "nvecs": None}
+
+    def job():
+        h = C.c_void_p()
+        _capi.check(L.gci_rkpq(C.byref(bstruct), cg.CHOL_ACCURACY_TIGHT, 0.0, 0, C.byref(h)))
+        nv = C.c_int64()
+        _capi.check(L.gci_query(h, C.byref(nv), None, None, None, None, None))
+        if state["rkab"] is None or state["nvecs"] != nv.value:
+            state["rkab"] = torch.empty(nv.value * NA * NB, dtype=torch.float64, device="cuda")
+            state["nvecs"] = nv.value
+        _capi.check(L.gci_rkab_device(h, C.c_void_p(c_dev.data_ptr()), nao, a0, a1, C.c_void_p(c_dev.data_ptr()),
+                                      nao, b0, b1, args.buffer_mb, prec, C.c_void_p(state["rkab"].data_ptr())))
+        st = np.zeros(8 + 300)
+        _capi.check(L.gci_stats(h, _capi.ptr(st), st.size))
+        tm = np.zeros(13)
+        _capi.check(L.gci_timings(h, _capi.ptr(tm), 13))
+        L.gci_free(h)
+        return st, tm
+
+    for _ in range(args.warmup):
+        job()
+    barrier()
+    n0 = C.c_int64()
+    _capi.check(L.gci_kernel_launches(C.byref(n0)))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record(lib_stream)
+        stats, times = [], []
+        for _ in range(args.steps):
+            st, tm = job()
+            stats.append(st)
+            times.append(tm)
+        ev1.record(lib_stream)
+        ev1.synchronize()
+        barrier()
+    n1 = C.c_int64()
+    _capi.check(L.gci_kernel_launches(C.byref(n1)))
+    t_dev = ev0.elapsed_time(ev1) * 1e-3
+    t_tensor = torch.tensor([t_dev], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_tensor, op=dist.ReduceOp.MAX)
+    t_max = float(t_tensor.item())
+    fl = flops.job_flops(stats[-1], 10)
+    flops_step = fl["total"]
+    value = flops_step * args.steps * world / t_max / 1e9
+
+    # ---- end to end through the public host API (pinned host buffers)
+    e2e = None
+    if args.e2e_steps > 0:
+        nv = state["nvecs"]
+        pin_c = torch.from_numpy(np.ascontiguousarray(Cm.T)).pin_memory()
+        pin_out = torch.empty(nv * NA * NB, dtype=torch.float64).pin_memory()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(lib_stream)
+        for _ in range(args.e2e_steps):
+            res = cg.chol_gammcor_Rkpq(tb, cg.CHOL_ACCURACY_TIGHT, materialize=False)
+            _capi.check(L.gci_rkab(res.handle.ptr, _capi.ptr(pin_c.numpy()), nao, a0, a1, _capi.ptr(pin_c.numpy()),
+                                   nao, b0, b1, args.buffer_mb, prec, _capi.ptr(pin_out.numpy())))
+            checksum = float(pin_out[:16].sum())
+            del res
+        e1.record(lib_stream)
+        e1.synchronize()
+        te = torch.tensor([e0.elapsed_time(e1) * 1e-3], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        te = float(te.item())
+        h2d = int(Cm.nbytes) + int(tb.CntrCoeffs.nbytes + tb.Exponents.nbytes + tb.AtomCoords.nbytes)
+        d2h = nv * NA * NB * 8
+        e2e = {"value": flops_step * args.e2e_steps * world / te / 1e9, "unit": "GFLOP/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "seconds_per_step": te / args.e2e_steps,
+               "checksum": checksum}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    tm = times[-1]
+    phases = {"vdiag": tm[0], "step1_eri": tm[1], "subtract_r": tm[2], "pivots": tm[3], "compress": tm[4],
+              "vjj_eri": tm[5], "potrf_trtri": tm[6], "fulldim_eri": tm[7], "invl_gemm": tm[8], "mo_gemm": tm[9]}
+    eri_t = tm[0] + tm[1] + tm[5] + tm[7]
+    gemm_t = tm[2] + tm[8] + tm[9]
+    peak64 = measured_fp64_peak(torch)
+    eri_rate = fl["eri"] / eri_t / 1e12 if eri_t > 0 else 0.0
+    roof = {"bound": "fp64", "kernel": "k_eri_class (all ERI stages)", "achieved": eri_rate, "peak": peak64,
+            "unit": "TFLOP/s", "frac": eri_rate / peak64 if peak64 else None, "traffic": None,
+            "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64; MEASURED_PEAKS.json has no FP64 figure)",
+            "eri_seconds": eri_t, "gemm_seconds": gemm_t}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        cpu = cpu_baseline_c1()
+    line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.config}: {len(mol.atoms)} atoms, NAO={nao}, tau={mol.tau}, "
+                                   f"Cholesky + AO->MO {NA}x{NB}",
+                       "precision": args.precision, "nvecs": state["nvecs"], "parallelism": f"replicas x{world}",
+                       "l2": "working set (Rkab, ERI buffers) far above L2 (126 MB)"},
+            "wall_s_per_step": t_max / args.steps, "gflop_per_step": flops_step / 1e9,
+            "eri_per_s": fl["integrals"] * args.steps * world / t_max, "phases_s": phases,
+            "gpu_launches": int(n1.value - n0.value), "roofline": roof, "e2e": e2e,
+            "clocks": clk.summary(), "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

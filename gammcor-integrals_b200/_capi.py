@@ -23,7 +23,8 @@ GCI_PREC_FP64, GCI_PREC_MIXED = 0, 1
 # every entry point declared in include/gci.h
 EXPORTS = ("gci_init", "gci_rkpq", "gci_query", "gci_copy_rkpq", "gci_copy_chol2data", "gci_pivot_order",
            "gci_rkab", "gci_timings", "gci_free", "gci_last_error", "gci_boys", "gci_spher_coeffs",
-           "gci_normalize_basis", "gci_eri_pairs")
+           "gci_normalize_basis", "gci_eri_pairs", "gci_rkab_device", "gci_stats", "gci_get_stream",
+           "gci_kernel_launches")
 
 _pd = C.POINTER(C.c_double)
 _pl = C.POINTER(C.c_int64)
@@ -68,6 +69,11 @@ def lib():
         L.gci_spher_coeffs.argtypes = [C.c_int, _pd]
         L.gci_normalize_basis.argtypes = [_i64, _i64, _pl, _pl, _pd, _pd, _pd, _i64, _pd, _i64]
         L.gci_eri_pairs.argtypes = [C.POINTER(gci_basis), C.c_double, _pd, _i64]
+        L.gci_rkab_device.argtypes = [C.c_void_p, C.c_void_p, _i64, _i64, _i64, C.c_void_p, _i64, _i64, _i64, _i64,
+                                      C.c_int, C.c_void_p]
+        L.gci_stats.argtypes = [C.c_void_p, _pd, C.c_int]
+        L.gci_get_stream.argtypes = [C.POINTER(C.c_void_p)]
+        L.gci_kernel_launches.argtypes = [_pl]
         _lib = L
     return _lib
 

@@ -227,6 +227,7 @@ cudaError_t launch_segmax(const double* D, const int64_t* loc, const int* dim, i
 {
     if (n <= 0) return cudaSuccess;
     k_segmax<<<grid_for(n, 256), 256, 0, s>>>(D, loc, dim, n, out);
+    count_launch();
     return cudaGetLastError();
 }
 cudaError_t launch_gather_rows(const double* src, int64_t lds, const int64_t* idx, int64_t nrows, int64_t ncols,
@@ -234,6 +235,7 @@ cudaError_t launch_gather_rows(const double* src, int64_t lds, const int64_t* id
 {
     if (nrows <= 0 || ncols <= 0) return cudaSuccess;
     k_gather_rows<<<grid_for(nrows * ncols, 256), 256, 0, s>>>(src, lds, idx, nrows, ncols, dst, ldd);
+    count_launch();
     return cudaGetLastError();
 }
 cudaError_t launch_gather_cols(const double* src, int64_t lds, const int* cols, int64_t nrows, int64_t ncols,
@@ -241,6 +243,7 @@ cudaError_t launch_gather_cols(const double* src, int64_t lds, const int* cols, 
 {
     if (nrows <= 0 || ncols <= 0) return cudaSuccess;
     k_gather_cols<<<grid_for(nrows * ncols, 256), 256, 0, s>>>(src, lds, cols, nrows, ncols, dst, ldd);
+    count_launch();
     return cudaGetLastError();
 }
 cudaError_t launch_pivot_batch(const double* Mbb, int nb, double* Db, double* Lb, int* piv, double* pdmax,
@@ -249,35 +252,41 @@ cudaError_t launch_pivot_batch(const double* Mbb, int nb, double* Db, double* Lb
     const size_t smem = sizeof(double) * (size_t)(nb + 32) + sizeof(int) * 32;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_pivot_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_pivot_batch<<<1, 1024, smem, s>>>(Mbb, nb, Db, Lb, piv, pdmax, npiv, nchol0, maxnchol, dmin);
+    count_launch();
     return cudaGetLastError();
 }
 cudaError_t launch_gather_pivrows(const double* Lb, int nb, const int* piv, int npiv, double* Lp, cudaStream_t s)
 {
     if (npiv <= 0) return cudaSuccess;
     k_gather_pivrows<<<grid_for((int64_t)npiv * npiv, 256), 256, 0, s>>>(Lb, nb, piv, npiv, Lp);
+    count_launch();
     return cudaGetLastError();
 }
 cudaError_t launch_tri_inv_lower(const double* L, int n, double* X, cudaStream_t s)
 {
     if (n <= 0) return cudaSuccess;
     k_tri_inv_lower<<<n < 148 * 8 ? n : 148 * 8, 128, 0, s>>>(L, n, X);
+    count_launch();
     return cudaGetLastError();
 }
 cudaError_t launch_downdate(double* D, const double* L, int64_t ld, int64_t n, int ncols, cudaStream_t s)
 {
     if (n <= 0 || ncols <= 0) return cudaSuccess;
     k_downdate<<<grid_for(n, 256), 256, 0, s>>>(D, L, ld, n, ncols);
+    count_launch();
     return cudaGetLastError();
 }
 cudaError_t launch_max(const double* v, int64_t n, double* out, cudaStream_t s)
 {
     k_max<<<1, 1024, 0, s>>>(v, n, out);
+    count_launch();
     return cudaGetLastError();
 }
 cudaError_t launch_zero_upper(double* A, int64_t n, cudaStream_t s)
 {
     if (n <= 0) return cudaSuccess;
     k_zero_upper<<<grid_for(n * n, 256), 256, 0, s>>>(A, n);
+    count_launch();
     return cudaGetLastError();
 }
 cudaError_t launch_unpack_rkpq(const double* R, int64_t nvecs, const int64_t* pq_col, const int* pq_ao, int64_t npq,
@@ -285,6 +294,7 @@ cudaError_t launch_unpack_rkpq(const double* R, int64_t nvecs, const int64_t* pq
 {
     if (npq <= 0 || kc <= 0) return cudaSuccess;
     k_unpack_rkpq<<<grid_for(npq * kc, 256), 256, 0, s>>>(R, nvecs, pq_col, pq_ao, npq, k0, kc, nao, U);
+    count_launch();
     return cudaGetLastError();
 }
 

@@ -1,132 +1,156 @@
 // eri_engine.cuh -- class-templated McMurchie-Davidson ERI kernel for sm_100a.
 //
 // One team of TW threads evaluates one contracted shell quartet (AB|CD) of a
-// canonical class (LA>=LB, LC>=LD, bra type >= ket type).  The algorithm is
+// canonical class (LA>=LB, LC>=LD, bra type >= ket type).  The arithmetic is
 // the reference's (src/integrals/Auto2e): the (LS|KS) matrix
 //   W(e,f) = sum_prims E^e_tuv (-1)^{tau+nu+phi} E^f R_{t+tau,u+nu,v+phi}
 // with single-centre Hermite coefficients (auto2e_WMatrix_part1.f90:743-812),
 // then the horizontal recurrence to (ab|cd) (auto2e_KetTransfer.f90) and the
-// Cartesian -> spherical/normalisation transforms (auto2e_SpherTransf.f90,
-// auto2e_Normalize_*).  The HRR is applied in its closed binomial form
-//   (a, b| = sum_{k<=b} C(b,k) (A-B)^{b-k} (a+k, 0|
-// so every output element is independent (no sequential recursion levels).
+// Cartesian -> spherical / normalisation transforms (auto2e_SpherTransf.f90,
+// auto2e_Normalize_*).  The sums are reordered for the GPU:
 //
-// Primitive-pair quantities (P, Rp, K_ab c_a c_b and the E^{e}_t tables) are
-// precomputed once per shell pair (k_pair_records) and read through the
-// read-only cache; R_tuv, the ket-transformed S(f,tuv) and the epilogue
-// tensors live in shared memory; the W accumulator lives in registers, spread
-// over the team's lanes.
+//  * for each ket primitive pair k, the bra side is contracted over all bra
+//    primitive pairs i in Hermite space first:
+//        T(e, g) = sum_i sum_{h in supp(e)} Eb_i(e, h) R_ik(h + g)
+//    with lane g of the team owning the ket Hermite index g = (tau,nu,phi)
+//    and T(e, g) for every bra function e in registers;
+//  * the ket transform W(e, f) += sum_g (-1)^|g| Ek_k(f, g) T(e, g) then runs
+//    once per ket primitive pair instead of once per primitive quartet;
+//  * the HRR uses its closed binomial form (a,b| = sum_k C(b,k)(A-B)^{b-k}(a+k,0|,
+//    so every output element of the epilogue is independent.
+//
+// R_tuv (Helgaker 9.9.18-20), the bra coefficient products and W live in
+// shared memory; all index tables are built in shared memory once per block.
 #pragma once
 #include "gci_common.h"
 #include "boys.cuh"
 
 namespace gci {
 
-constexpr int kCartTab = cart_off(kMaxPairL + 3);   // levels 0..kMaxPairL+2
-constexpr int kHermTab = herm_n(kMaxDerivLT);
-
-struct DeviceTables {
-    unsigned char cart[3 * kCartTab];
-    unsigned char herm[3 * kHermTab];
-    double binom[8][8];
-};
-
-// One copy per translation unit; filled by upload_device_tables() below.
-static __constant__ DeviceTables c_tab;
-
-static inline cudaError_t upload_device_tables()
+// ------------------------------------------------------------ compile-time index helpers
+GCI_HD constexpr int cart_level(int g) { int l = 0; while (cart_off(l + 1) <= g) ++l; return l; }
+GCI_HD constexpr int cart_x(int g) { int l = cart_level(g), p = g - cart_off(l), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return l - s; }
+GCI_HD constexpr int cart_z(int g) { int l = cart_level(g), p = g - cart_off(l), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return p - s * (s + 1) / 2; }
+GCI_HD constexpr int cart_y(int g) { return cart_level(g) - cart_x(g) - cart_z(g); }
+GCI_HD constexpr int herm_level(int h) { int n = 0; while (herm_n(n) <= h) ++n; return n; }
+GCI_HD constexpr int herm_v(int h) { int n = herm_level(h), p = h - (n > 0 ? herm_n(n - 1) : 0), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return p - s * (s + 1) / 2; }
+GCI_HD constexpr int herm_u(int h) { int n = herm_level(h), p = h - (n > 0 ? herm_n(n - 1) : 0), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return s - (p - s * (s + 1) / 2); }
+GCI_HD constexpr int herm_t(int h) { return herm_level(h) - herm_u(h) - herm_v(h); }
+GCI_HD constexpr int supp_size(int g) { return (cart_x(g) + 1) * (cart_y(g) + 1) * (cart_z(g) + 1); }
+GCI_HD constexpr int cmax(int a, int b) { return a > b ? a : b; }
+GCI_HD constexpr double c_binom(int n, int k)
 {
-    DeviceTables h{};
-    for (int l = 0; l <= kMaxPairL + 2; ++l) {
-        int i = cart_off(l);
-        for (int x = l; x >= 0; --x)
-            for (int y = l - x; y >= 0; --y) {
-                h.cart[3 * i + 0] = (unsigned char)x;
-                h.cart[3 * i + 1] = (unsigned char)y;
-                h.cart[3 * i + 2] = (unsigned char)(l - x - y);
-                ++i;
-            }
-    }
-    for (int n = 0; n <= kMaxDerivLT; ++n)
-        for (int s = 0; s <= n; ++s)
-            for (int v = 0; v <= s; ++v) {
-                int u = s - v, t = n - s;
-                int i = herm_idx(t, u, v);
-                h.herm[3 * i + 0] = (unsigned char)t;
-                h.herm[3 * i + 1] = (unsigned char)u;
-                h.herm[3 * i + 2] = (unsigned char)v;
-            }
-    for (int n = 0; n < 8; ++n)
-        for (int k = 0; k < 8; ++k) {
-            double b = 0.0;
-            if (k <= n) { b = 1.0; for (int i = 0; i < k; ++i) b = b * (n - i) / (i + 1); }
-            h.binom[n][k] = b;
-        }
-    return cudaMemcpyToSymbol(c_tab, &h, sizeof(h));
+    double b = 1.0;
+    for (int i = 0; i < k; ++i) b = b * (n - i) / (i + 1);
+    return b;
 }
-
-template <int TW, int TPB>
-__device__ __forceinline__ void team_sync()
-{
-    if constexpr (TW == TPB && TPB > 32) {
-        __syncthreads();
-    } else if constexpr (TW == 32) {
-        __syncwarp();
-    } else if constexpr (TW > 1) {
-        const unsigned lane_in_warp = threadIdx.x & 31u;
-        const unsigned base = (lane_in_warp / TW) * TW;
-        const unsigned mask = ((TW == 32) ? 0xffffffffu : ((1u << TW) - 1u)) << base;
-        __syncwarp(mask);
-    }
-}
-
-constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
 template <int LA, int LB, int LC, int LD>
 struct EriShape {
     static constexpr int L1 = LA + LB, L2 = LC + LD, LT = L1 + L2;
     static constexpr int E0 = cart_off(LA), NE = cart_off(L1 + 1) - E0;
     static constexpr int F0 = cart_off(LC), NF = cart_off(L2 + 1) - F0;
-    static constexpr int HT = herm_n(LT), H1 = herm_n(L1);
+    static constexpr int HT = herm_n(LT), H1 = herm_n(L1), H2 = herm_n(L2);
     static constexpr int nA = ncart(LA), nB = ncart(LB), nC = ncart(LC), nD = ncart(LD);
     static constexpr int RSA = pp_record(L1), RSB = pp_record(L2);
-    static constexpr int SZ_MAIN = 2 * HT + NF * H1;
+    static constexpr int cb_count()
+    {
+        int n = 0;
+        for (int e = 0; e < NE; ++e) n += supp_size(E0 + e);
+        return n;
+    }
+    static constexpr int NCB = cb_count();
+    // team scratch (doubles): W, R ping-pong, bra products, T spill
+    static constexpr int O_W = 0, O_RA = NE * NF, O_RB = O_RA + HT, O_CB = O_RB + HT, O_TT = O_CB + NCB;
+    static constexpr int SZ_MAIN = O_TT + NE * H2;
+    // epilogue ping-pong over the same scratch (P0 holds W on entry)
     static constexpr int SZ_P0 = cmax(NE * NF, cmax(NE * nC * nD, nA * nB * nC * nD));
     static constexpr int SZ_P1 = cmax(NE * nC * nD, nA * nB * nC * nD);
     static constexpr int SZ_TEAM = cmax(SZ_MAIN, SZ_P0 + SZ_P1);
+    // per-block tables (ints)
+    static constexpr int TAB_CB = NCB;            // packed E-table offsets of each bra product
+    static constexpr int TAB_RIDX = H2 * H1;      // R index of h + g
+    static constexpr int TAB_HERM = HT;           // packed (t,u,v) of each Hermite index
+    static constexpr int TAB_INTS = TAB_CB + TAB_RIDX + TAB_HERM;
 };
 
-// Shared-memory view of one team's scratch: AoS per team for TW > 1,
-// interleaved (element-major) across teams for TW == 1 so that neighbouring
-// threads touch neighbouring words.
-template <int TW, int TPB, int SZ>
-struct TeamMem {
-    static constexpr int NT = TPB / TW;
-    static constexpr int STRIDE = (TW == 1) ? NT : 1;
-    static constexpr int TEAM_SZ = (TW == 1) ? 1 : (SZ | 1);
-    double* base;
-    __device__ __forceinline__ double& operator[](int k) const { return base[k * STRIDE]; }
-    __device__ __forceinline__ TeamMem shifted(int k) const { return TeamMem{base + k * STRIDE}; }
-    static constexpr size_t bytes() { return sizeof(double) * (size_t)((TW == 1) ? NT * SZ : NT * TEAM_SZ); }
+// Team geometry: TW lanes own the ket Hermite indices (TW >= H2).  Teams of at
+// most 32 lanes are packed floor(32/TW) per warp in one-warp blocks; wider
+// teams fill a block of their own.
+template <int LA, int LB, int LC, int LD>
+struct EriTeam {
+    using S = EriShape<LA, LB, LC, LD>;
+    static constexpr int TW = S::H2 <= 32 ? S::H2 : 32 * ((S::H2 + 31) / 32);
+    static constexpr int TPB = TW <= 32 ? 32 : TW;
+    static constexpr int TEAM_SZ = S::SZ_TEAM | 1;
+    // teams per block: as many as fit in a warp, within ~96 KB of team scratch
+    static constexpr int NT_WARP = TW <= 32 ? 32 / TW : 1;
+    static constexpr int NT_SMEM = (int)((96 * 1024) / (sizeof(double) * TEAM_SZ));
+    static constexpr int NT = NT_WARP < NT_SMEM ? NT_WARP : (NT_SMEM > 0 ? NT_SMEM : 1);
+    static constexpr size_t smem_bytes()
+    {
+        return sizeof(double) * (size_t)NT * TEAM_SZ + sizeof(int) * (size_t)S::TAB_INTS;
+    }
 };
+
+template <int TW, int TPB>
+__device__ __forceinline__ void team_sync()
+{
+    if constexpr (TW > 32) {
+        __syncthreads();
+    } else if constexpr (TW == 32) {
+        __syncwarp();
+    } else if constexpr (TW > 1) {
+        const unsigned base = (threadIdx.x / TW) * TW;
+        __syncwarp(((1u << TW) - 1u) << base);
+    }
+}
 
 __device__ __forceinline__ void set_err(int* err, int code)
 {
     if (err) atomicCAS(err, 0, code);
 }
 
-template <int LA, int LB, int LC, int LD, int TW, int TPB>
-__global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(EriTeam<LA, LB, LC, LD>::TPB)
+k_eri_class(const EriArgs a)
 {
     using S = EriShape<LA, LB, LC, LD>;
-    using TM = TeamMem<TW, TPB, S::SZ_TEAM>;
-    constexpr int NT = TPB / TW;
-    constexpr int NWORK = S::NE * S::NF;
-    constexpr int WPL = (NWORK + TW - 1) / TW;
+    using G = EriTeam<LA, LB, LC, LD>;
+    constexpr int TW = G::TW, TPB = G::TPB, NT = G::NT;
     extern __shared__ double smem[];
+    int* tab = reinterpret_cast<int*>(smem + (size_t)NT * G::TEAM_SZ);
+    int* tab_cb = tab;                       // (x | y << 8 | z << 16) offsets into the E tables
+    int* tab_ridx = tab + S::TAB_CB;         // [g][h] -> herm_idx(h + g)
+    int* tab_herm = tab_ridx + S::TAB_RIDX;  // t | u << 8 | v << 16
+
+    // ---- per-block tables
+    for (int c = threadIdx.x; c < S::NCB; c += TPB) {
+        int e = 0, off = 0;
+        while (off + supp_size(S::E0 + e) <= c) { off += supp_size(S::E0 + e); ++e; }
+        const int g = S::E0 + e;
+        const int ex = cart_x(g), ey = cart_y(g);
+        const int r = c - off;                       // order: v outer, u, t inner
+        const int t = r % (ex + 1), u = (r / (ex + 1)) % (ey + 1), v = r / ((ex + 1) * (ey + 1));
+        const int ez = cart_z(g);
+        tab_cb[c] = (ex * (ex + 1) / 2 + t) | ((ey * (ey + 1) / 2 + u) << 8) | ((ez * (ez + 1) / 2 + v) << 16);
+    }
+    for (int c = threadIdx.x; c < S::TAB_RIDX; c += TPB) {
+        const int g = c / S::H1, h = c - g * S::H1;
+        tab_ridx[c] = herm_idx(herm_t(h) + herm_t(g), herm_u(h) + herm_u(g), herm_v(h) + herm_v(g));
+    }
+    for (int c = threadIdx.x; c < S::HT; c += TPB) tab_herm[c] = herm_t(c) | (herm_u(c) << 8) | (herm_v(c) << 16);
+    __syncthreads();
+
     const int team = threadIdx.x / TW;
-    const int lane = threadIdx.x % TW;
-    const TM ts{smem + ((TW == 1) ? team : team * TM::TEAM_SZ)};
+    const int lane = threadIdx.x - team * TW;
+    if (team >= NT) return;   // lanes left over when TW does not divide 32
+    double* ts = smem + (size_t)team * G::TEAM_SZ;
+    double* RA = ts + S::O_RA;
+    double* RB = ts + S::O_RB;
+    double* CBv = ts + S::O_CB;
+    double* TT = ts + S::O_TT;
+    double* WW = ts + S::O_W;
 
     const int64_t ntasks = (a.mode == kModeDiagonal) ? a.nbra : a.nbra * a.nket;
     const int64_t stride = (int64_t)gridDim.x * NT;
@@ -147,32 +171,29 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
         const int nbp = pb.nprim1 * pb.nprim2;
         const int nkp = pk.nprim1 * pk.nprim2;
 
-        double w[WPL];
-#pragma unroll
-        for (int i = 0; i < WPL; ++i) w[i] = 0.0;
-
-        const TM RA = ts;
-        const TM RB = ts.shifted(S::HT);
-        const TM SS = ts.shifted(2 * S::HT);
+        for (int w = lane; w < S::NE * S::NF; w += TW) WW[w] = 0.0;
+        // lane -> ket Hermite index g and the R indices it reads
+        const bool gl = lane < S::H2;
+        const int* ridx = tab_ridx + (gl ? lane : 0) * S::H1;
 
         for (int kp = 0; kp < nkp; ++kp) {
             const double* __restrict__ K = rk + (size_t)kp * S::RSB;
             const double Q = __ldg(K + 0);
             const double qx = __ldg(K + 1), qy = __ldg(K + 2), qz = __ldg(K + 3);
             const double pcd = __ldg(K + 4);
-            const double* __restrict__ Ecx = K + 8;
-            const double* __restrict__ Ecy = Ecx + tri(S::L2);
-            const double* __restrict__ Ecz = Ecy + tri(S::L2);
+            double T[S::NE];
+#pragma unroll
+            for (int e = 0; e < S::NE; ++e) T[e] = 0.0;
+
             for (int bp = 0; bp < nbp; ++bp) {
                 const double* __restrict__ Bp = rb + (size_t)bp * S::RSA;
                 const double P = __ldg(Bp + 0);
                 const double X = __ldg(Bp + 1) - qx, Y = __ldg(Bp + 2) - qy, Z = __ldg(Bp + 3) - qz;
-                const double pab = __ldg(Bp + 4);
                 const double PQ = P * Q;
                 const double den = P + Q + a.kappa * PQ;
                 const double alpha = PQ / den;
                 // 2 pi^{5/2} / (PQ sqrt(P+Q+kappa PQ)) (auto2e_WMatrix_part1.f90:134)
-                const double pref = 34.986836655249725 / (PQ * sqrt(den)) * pab * pcd;
+                const double pref = 34.986836655249725 / (PQ * sqrt(den)) * __ldg(Bp + 4) * pcd;
                 double F[S::LT + 1];
                 boys_fm<S::LT>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
                 {
@@ -181,15 +202,27 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
 #pragma unroll
                     for (int m = 0; m <= S::LT; ++m) { F[m] *= pw; pw *= m2a; }
                 }
-                // ---- Hermite Coulomb integrals R^{(0)}_{tuv}, t+u+v <= LT ----
-                TM cur = RA, nxt = RB;
+                // bra coefficient products Eb(e,h) = Ex Ey Ez (this bra primitive pair)
+                {
+                    const double* __restrict__ Ebx = Bp + 8;
+                    const double* __restrict__ Eby = Ebx + tri(S::L1);
+                    const double* __restrict__ Ebz = Eby + tri(S::L1);
+                    for (int c = lane; c < S::NCB; c += TW) {
+                        const int o = tab_cb[c];
+                        CBv[c] = __ldg(Ebx + (o & 0xff)) * __ldg(Eby + ((o >> 8) & 0xff)) * __ldg(Ebz + (o >> 16));
+                    }
+                }
+                // Hermite Coulomb integrals R^{(0)}_{tuv}, t+u+v <= LT
+                double* cur = RA;
+                double* nxt = RB;
                 if (lane == 0) cur[0] = F[S::LT];
                 team_sync<TW, TPB>();
 #pragma unroll
                 for (int j = S::LT - 1; j >= 0; --j) {
                     const int nent = herm_n(S::LT - j);
                     for (int h = lane; h < nent; h += TW) {
-                        const int t = c_tab.herm[3 * h], u = c_tab.herm[3 * h + 1], v = c_tab.herm[3 * h + 2];
+                        const int p = tab_herm[h];
+                        const int t = p & 0xff, u = (p >> 8) & 0xff, v = p >> 16;
                         double r;
                         if (t > 0) {
                             r = X * cur[herm_idx(t - 1, u, v)];
@@ -206,70 +239,90 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
                         nxt[h] = r;
                     }
                     team_sync<TW, TPB>();
-                    TM tmp = cur; cur = nxt; nxt = tmp;
+                    double* tmp = cur; cur = nxt; nxt = tmp;
                 }
-                // ---- ket Hermite -> Cartesian: S(f, tuv), tuv in bra range ----
-                for (int idx = lane; idx < S::NF * S::H1; idx += TW) {
-                    const int f = idx / S::H1, h = idx - f * S::H1;
-                    const int fg = S::F0 + f;
-                    const int fx = c_tab.cart[3 * fg], fy = c_tab.cart[3 * fg + 1], fz = c_tab.cart[3 * fg + 2];
-                    const int t = c_tab.herm[3 * h], u = c_tab.herm[3 * h + 1], v = c_tab.herm[3 * h + 2];
-                    double acc = 0.0;
-                    for (int p3 = 0; p3 <= fz; ++p3) {
-                        const double ez = __ldg(Ecz + fz * (fz + 1) / 2 + p3) * ((p3 & 1) ? -1.0 : 1.0);
-                        double a2 = 0.0;
-                        for (int p2 = 0; p2 <= fy; ++p2) {
-                            const double ey = __ldg(Ecy + fy * (fy + 1) / 2 + p2) * ((p2 & 1) ? -1.0 : 1.0);
-                            double a1 = 0.0;
-                            for (int p1 = 0; p1 <= fx; ++p1) {
-                                const double ex = __ldg(Ecx + fx * (fx + 1) / 2 + p1) * ((p1 & 1) ? -1.0 : 1.0);
-                                a1 += ex * cur[herm_idx(t + p1, u + p2, v + p3)];
-                            }
-                            a2 += ey * a1;
-                        }
-                        acc += ez * a2;
-                    }
-                    SS[idx] = acc;
-                }
-                team_sync<TW, TPB>();
-                // ---- bra Hermite -> Cartesian, accumulate W(e,f) ----
-                const double* __restrict__ Ebx = Bp + 8;
-                const double* __restrict__ Eby = Ebx + tri(S::L1);
-                const double* __restrict__ Ebz = Eby + tri(S::L1);
+                // T(e, g) += sum_{h in supp(e)} Eb(e, h) R(h + g)
+                if (gl) {
+                    if constexpr (S::H1 <= 56) {
+                        double Rl[S::H1];
 #pragma unroll
-                for (int i = 0; i < WPL; ++i) {
-                    const int idx = lane + i * TW;
-                    if (idx < NWORK) {
-                        const int e = idx / S::NF, f = idx - e * S::NF;
-                        const int eg = S::E0 + e;
-                        const int ex = c_tab.cart[3 * eg], ey = c_tab.cart[3 * eg + 1], ez = c_tab.cart[3 * eg + 2];
-                        const TM Sf = SS.shifted(f * S::H1);
-                        double acc = 0.0;
-                        for (int v = 0; v <= ez; ++v) {
-                            double a2 = 0.0;
-                            for (int u = 0; u <= ey; ++u) {
-                                double a1 = 0.0;
-                                for (int t = 0; t <= ex; ++t)
-                                    a1 += __ldg(Ebx + ex * (ex + 1) / 2 + t) * Sf[herm_idx(t, u, v)];
-                                a2 += __ldg(Eby + ey * (ey + 1) / 2 + u) * a1;
-                            }
-                            acc += __ldg(Ebz + ez * (ez + 1) / 2 + v) * a2;
+                        for (int h = 0; h < S::H1; ++h) Rl[h] = cur[ridx[h]];
+                        int c = 0;
+#pragma unroll
+                        for (int e = 0; e < S::NE; ++e) {
+                            const int g = S::E0 + e;
+                            double acc = T[e];
+#pragma unroll
+                            for (int v = 0; v <= cart_z(g); ++v)
+#pragma unroll
+                                for (int u = 0; u <= cart_y(g); ++u)
+#pragma unroll
+                                    for (int t = 0; t <= cart_x(g); ++t) {
+                                        acc += CBv[c] * Rl[herm_idx(t, u, v)];
+                                        ++c;
+                                    }
+                            T[e] = acc;
                         }
-                        w[i] += acc;
+                    } else {
+                        int c = 0;
+#pragma unroll
+                        for (int e = 0; e < S::NE; ++e) {
+                            const int g = S::E0 + e;
+                            double acc = T[e];
+#pragma unroll
+                            for (int v = 0; v <= cart_z(g); ++v)
+#pragma unroll
+                                for (int u = 0; u <= cart_y(g); ++u)
+#pragma unroll
+                                    for (int t = 0; t <= cart_x(g); ++t) {
+                                        acc += CBv[c] * cur[ridx[herm_idx(t, u, v)]];
+                                        ++c;
+                                    }
+                            T[e] = acc;
+                        }
                     }
                 }
                 team_sync<TW, TPB>();
             }
+            // ---- ket transform for this ket primitive pair:
+            //      W(e, f) += sum_{g in supp(f)} (-1)^{tau+nu+phi} Ek(f, g) T(e, g)
+            if (gl) {
+#pragma unroll
+                for (int e = 0; e < S::NE; ++e) TT[e * S::H2 + lane] = T[e];
+            }
+            team_sync<TW, TPB>();
+            {
+                const double* __restrict__ Ekx = K + 8;
+                const double* __restrict__ Eky = Ekx + tri(S::L2);
+                const double* __restrict__ Ekz = Eky + tri(S::L2);
+                for (int f = lane; f < S::NF; f += TW) {
+                    const int fg = S::F0 + f;
+                    const int fx = cart_x(fg), fy = cart_y(fg), fz = cart_z(fg);
+                    double wcol[S::NE];
+#pragma unroll
+                    for (int e = 0; e < S::NE; ++e) wcol[e] = WW[e * S::NF + f];
+                    for (int p3 = 0; p3 <= fz; ++p3) {
+                        const double cz = __ldg(Ekz + fz * (fz + 1) / 2 + p3) * ((p3 & 1) ? -1.0 : 1.0);
+                        for (int p2 = 0; p2 <= fy; ++p2) {
+                            const double cyz = cz * __ldg(Eky + fy * (fy + 1) / 2 + p2) * ((p2 & 1) ? -1.0 : 1.0);
+                            for (int p1 = 0; p1 <= fx; ++p1) {
+                                const double c = cyz * __ldg(Ekx + fx * (fx + 1) / 2 + p1) * ((p1 & 1) ? -1.0 : 1.0);
+                                const int g = herm_idx(p1, p2, p3);
+#pragma unroll
+                                for (int e = 0; e < S::NE; ++e) wcol[e] += c * TT[e * S::H2 + g];
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int e = 0; e < S::NE; ++e) WW[e * S::NF + f] = wcol[e];
+                }
+            }
+            team_sync<TW, TPB>();
         }
 
         // ================= epilogue: HRR + transforms + scatter =================
-        const TM P0 = ts;
-        const TM P1 = ts.shifted(S::SZ_P0);
-#pragma unroll
-        for (int i = 0; i < WPL; ++i) {
-            const int idx = lane + i * TW;
-            if (idx < NWORK) P0[idx] = w[i];
-        }
+        double* P0 = WW;                 // holds W(e, f) on entry
+        double* P1 = WW + S::SZ_P0;
         const int A = pb.s1, B = pb.s2, C = pk.s1, D = pk.s2;
         const double ABx = __ldg(a.sh_xyz + 3 * A) - __ldg(a.sh_xyz + 3 * B);
         const double ABy = __ldg(a.sh_xyz + 3 * A + 1) - __ldg(a.sh_xyz + 3 * B + 1);
@@ -279,15 +332,14 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
         const double CDz = __ldg(a.sh_xyz + 3 * C + 2) - __ldg(a.sh_xyz + 3 * D + 2);
         const int nfA = __ldg(a.sh_nfunc + A), nfB = __ldg(a.sh_nfunc + B);
         const int nfC = __ldg(a.sh_nfunc + C), nfD = __ldg(a.sh_nfunc + D);
-        team_sync<TW, TPB>();
         // 1) ket HRR: X[e][c][d] (P1)
         for (int idx = lane; idx < S::NE * S::nC * S::nD; idx += TW) {
             const int e = idx / (S::nC * S::nD);
             const int r = idx - e * (S::nC * S::nD);
             const int c = r / S::nD, d = r - c * S::nD;
             const int cg = cart_off(LC) + c, dg = cart_off(LD) + d;
-            const int cx = c_tab.cart[3 * cg], cy = c_tab.cart[3 * cg + 1], cz = c_tab.cart[3 * cg + 2];
-            const int dx = c_tab.cart[3 * dg], dy = c_tab.cart[3 * dg + 1], dz = c_tab.cart[3 * dg + 2];
+            const int cy = cart_y(cg), cz = cart_z(cg);
+            const int dx = cart_x(dg), dy = cart_y(dg), dz = cart_z(dg);
             double acc = 0.0;
             double pz = 1.0;
             for (int kz = dz; kz >= 0; --kz) {
@@ -295,10 +347,8 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
                 for (int ky = dy; ky >= 0; --ky) {
                     double px = 1.0;
                     for (int kx = dx; kx >= 0; --kx) {
-                        const int lev = LC + kx + ky + kz;
-                        const int fi = cart_off(lev) + cart_pos(cy + ky, cz + kz) - S::F0;
-                        acc += c_tab.binom[dx][kx] * c_tab.binom[dy][ky] * c_tab.binom[dz][kz] * px * py * pz *
-                               P0[e * S::NF + fi];
+                        const int fi = cart_off(LC + kx + ky + kz) + cart_pos(cy + ky, cz + kz) - S::F0;
+                        acc += c_binom(dx, kx) * c_binom(dy, ky) * c_binom(dz, kz) * px * py * pz * P0[e * S::NF + fi];
                         px *= CDx;
                     }
                     py *= CDy;
@@ -328,8 +378,7 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
             const int mc = q / nfD, md = q - mc * nfD;
             double acc = 0.0;
 #pragma unroll
-            for (int c = 0; c < S::nC; ++c)
-                acc += __ldg(TC + mc * S::nC + c) * P0[(e * S::nC + c) * nfD + md];
+            for (int c = 0; c < S::nC; ++c) acc += __ldg(TC + mc * S::nC + c) * P0[(e * S::nC + c) * nfD + md];
             P1[idx] = acc;
         }
         team_sync<TW, TPB>();
@@ -338,8 +387,8 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
             const int ab = idx / nq, q = idx - ab * nq;
             const int ai = ab / S::nB, bi = ab - ai * S::nB;
             const int ag = cart_off(LA) + ai, bg = cart_off(LB) + bi;
-            const int ax = c_tab.cart[3 * ag], ay = c_tab.cart[3 * ag + 1], az = c_tab.cart[3 * ag + 2];
-            const int bx = c_tab.cart[3 * bg], by = c_tab.cart[3 * bg + 1], bz = c_tab.cart[3 * bg + 2];
+            const int ay = cart_y(ag), az = cart_z(ag);
+            const int bx = cart_x(bg), by = cart_y(bg), bz = cart_z(bg);
             double acc = 0.0;
             double pz = 1.0;
             for (int kz = bz; kz >= 0; --kz) {
@@ -347,10 +396,8 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
                 for (int ky = by; ky >= 0; --ky) {
                     double px = 1.0;
                     for (int kx = bx; kx >= 0; --kx) {
-                        const int lev = LA + kx + ky + kz;
-                        const int ei = cart_off(lev) + cart_pos(ay + ky, az + kz) - S::E0;
-                        acc += c_tab.binom[bx][kx] * c_tab.binom[by][ky] * c_tab.binom[bz][kz] * px * py * pz *
-                               P1[ei * nq + q];
+                        const int ei = cart_off(LA + kx + ky + kz) + cart_pos(ay + ky, az + kz) - S::E0;
+                        acc += c_binom(bx, kx) * c_binom(by, ky) * c_binom(bz, kz) * px * py * pz * P1[ei * nq + q];
                         px *= ABx;
                     }
                     py *= ABy;
@@ -371,8 +418,6 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
         }
         team_sync<TW, TPB>();
         // 6) T_A on a and scatter
-        const ShellPairDev& pbr = pb;
-        const ShellPairDev& pkr = pk;
         const int nout = nfA * nfB * nq;
         for (int idx = lane; idx < nout; idx += TW) {
             const int mm = idx / nq, q = idx - mm * nq;
@@ -382,8 +427,8 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
 #pragma unroll
             for (int ai = 0; ai < S::nA; ++ai) val += __ldg(TA + ma * S::nA + ai) * P1[(ai * nfB + mb) * nq + q];
             // canonical -> stored orientation of each pair
-            const int fb = pbr.swap ? (mb + nfB * ma) : (ma + nfA * mb);
-            const int fk = pkr.swap ? (md + nfD * mc) : (mc + nfC * md);
+            const int fb = pb.swap ? (mb + nfB * ma) : (ma + nfA * mb);
+            const int fk = pk.swap ? (md + nfD * mc) : (mc + nfC * md);
             const int rowf = a.swap_bk ? fk : fb;
             const int colf = a.swap_bk ? fb : fk;
             if (a.mode == kModeProduct) {
@@ -396,8 +441,8 @@ __global__ void __launch_bounds__(TPB) k_eri_class(const EriArgs a)
                     if (row >= 0) a.out[row] = val;
                 }
             } else {
-                // dense symmetric AO-pair layout [p][q][j], the stored bra pair gives (p,q)
-                const ShellPairDev& ps = a.swap_bk ? pkr : pbr;
+                // dense symmetric AO-pair layout [p][q][j]; the stored bra pair gives (p, q)
+                const ShellPairDev& ps = a.swap_bk ? pk : pb;
                 const int first = ps.swap ? ps.s2 : ps.s1;
                 const int second = ps.swap ? ps.s1 : ps.s2;
                 const int n1 = __ldg(a.sh_nfunc + first);

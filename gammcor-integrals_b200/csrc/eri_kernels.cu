@@ -1,6 +1,6 @@
 // eri_kernels.cu -- instantiation and dispatch of the class-templated ERI
 // kernels, the primitive-pair record kernel and the Boys self-test kernel.
-#include "eri_engine.cuh"
+#include "eri_classes.cuh"
 #include "gci_runtime.h"
 
 namespace gci {
@@ -64,73 +64,18 @@ __global__ void k_boys_eval(int m, int64_t n, const double* __restrict__ x, cons
     }
 }
 
-// ---------------------------------------------------------------------------
-// Per-class launch configuration: team width TW (threads per shell quartet)
-// from the size of the W accumulator, one block of TPB threads.
-// ---------------------------------------------------------------------------
-constexpr int type_lhi(int t) { return t >= 6 ? 3 : (t >= 3 ? 2 : (t >= 1 ? 1 : 0)); }
-constexpr int type_llo(int t) { return t - pair_type(type_lhi(t), 0); }
-
-template <int LA, int LB, int LC, int LD>
-struct EriConfig {
-    using S = EriShape<LA, LB, LC, LD>;
-    static constexpr int NW = S::NE * S::NF;
-    static constexpr int TW0 = NW <= 16 ? 1 : (NW <= 96 ? 4 : (NW <= 400 ? 16 : (NW <= 1600 ? 32 : 128)));
-    static constexpr size_t team_bytes = sizeof(double) * (size_t)((S::SZ_TEAM | 1));
-    // widen the team until one block's shared memory stays within ~100 KB
-    static constexpr int next_tw(int tw) { return tw == 16 ? 32 : (tw == 32 ? 128 : tw * 2); }
-    static constexpr int pick(int tw)
-    {
-        return (tw >= 128) ? 128 : (((size_t)(128 / tw) * team_bytes <= 100 * 1024) ? tw : pick(next_tw(tw)));
-    }
-    static constexpr int TW = pick(TW0);
-    static constexpr int TPB = 128;
-};
-
-template <int TB, int TK>
-static void launch_class(const EriArgs& args, cudaStream_t st)
-{
-    constexpr int LA = type_lhi(TB), LB = type_llo(TB), LC = type_lhi(TK), LD = type_llo(TK);
-    using Cfg = EriConfig<LA, LB, LC, LD>;
-    using S = EriShape<LA, LB, LC, LD>;
-    using TM = TeamMem<Cfg::TW, Cfg::TPB, S::SZ_TEAM>;
-    constexpr int NT = Cfg::TPB / Cfg::TW;
-    const size_t smem = TM::bytes();
-    auto kern = k_eri_class<LA, LB, LC, LD, Cfg::TW, Cfg::TPB>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-    }
-    const int64_t ntasks = (args.mode == kModeDiagonal) ? args.nbra : args.nbra * args.nket;
-    if (ntasks <= 0) return;
-    int64_t blocks = (ntasks + NT - 1) / NT;
-    const int64_t cap = 148LL * 32;
-    if (blocks > cap) blocks = cap;
-    kern<<<(unsigned)blocks, Cfg::TPB, smem, st>>>(args);
-}
-
-using LaunchFn = void (*)(const EriArgs&, cudaStream_t);
 static LaunchFn g_launch[kNumPairTypes][kNumPairTypes];
-
-template <int TB, int TK>
-struct Register {
-    static void run()
-    {
-        g_launch[TB][TK] = &launch_class<TB, TK>;
-        if constexpr (TK > 0) Register<TB, TK - 1>::run();
-        else if constexpr (TB > 0) Register<TB - 1, TB - 1>::run();
-    }
-};
 
 cudaError_t eri_module_init()
 {
     static bool done = false;
     if (done) return cudaSuccess;
-    Register<kNumPairTypes - 1, kNumPairTypes - 1>::run();
-    cudaError_t e = upload_device_tables();
-    if (e == cudaSuccess) done = true;
-    return e;
+    register_eri_classes_a(g_launch);
+    register_eri_classes_b(g_launch);
+    register_eri_classes_c(g_launch);
+    register_eri_classes_d(g_launch);
+    done = true;
+    return cudaSuccess;
 }
 
 int eri_team_width(int tb, int tk)
@@ -143,6 +88,7 @@ cudaError_t eri_launch(int tb, int tk, const EriArgs& args, cudaStream_t st)
 {
     if (tb < 0 || tk < 0 || tb >= kNumPairTypes || tk >= kNumPairTypes || tb < tk) return cudaErrorInvalidValue;
     g_launch[tb][tk](args, st);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -152,6 +98,7 @@ cudaError_t pair_records_launch(const ShellPairDev* pairs, int npairs, const dou
     if (npairs <= 0) return cudaSuccess;
     int blocks = npairs < 148 * 64 ? npairs : 148 * 64;
     k_pair_records<<<blocks, 64, 0, st>>>(pairs, npairs, xyz, poff, exps, coefs, pp);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -161,6 +108,7 @@ cudaError_t boys_eval_launch(int m, int64_t n, const double* x, const double* ta
     int64_t blocks = (n + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
     k_boys_eval<<<(unsigned)blocks, 256, 0, st>>>(m, n, x, table, out);
+    count_launch();
     return cudaGetLastError();
 }
 

@@ -13,6 +13,7 @@
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -62,6 +63,11 @@ static int guarded(F&& f)
         return GCI_ERR_ARG;
     }
 }
+
+// ------------------------------------------------------------------ launch counter
+static std::atomic<int64_t> g_launches{0};
+void count_launch(int64_t n) { g_launches += n; }
+int64_t launches() { return g_launches.load(); }
 
 // ------------------------------------------------------------------ device buffers
 template <class T>
@@ -290,6 +296,8 @@ struct PairMap {
     }
 };
 
+enum GemmPhase { kGemmSubtractR = 0, kGemmLnew, kGemmPotrf, kGemmInvL, kGemmMo, kNumGemm };
+
 struct Handle;
 static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<int>& ket, int mode, PairMap* rows,
                     PairMap* cols, double* out, int64_t ldo, int64_t jcount = 0);
@@ -318,6 +326,9 @@ struct Handle {
     PairMap pivmap;                        // pivot columns, by pair id
     PhaseTimer timer;
     double t_rkpq = 0.0, t_rkab = 0.0;
+    // work counters: GEMM flops per phase and ERI work per canonical class
+    double gemm_flops[kNumGemm] = {0};
+    double eri_stats[kNumPairTypes][kNumPairTypes][3] = {};   // shell quartets, primitive quartets, integrals
     // scratch reused across ERI launches
     DVec<int> d_bra, d_ket;
 };
@@ -410,10 +421,29 @@ static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<in
     a.kappa = H.kappa;
     a.boys = C.boys.p;
     a.err = C.err.p;
+    auto sums = [&](const std::vector<int>& g, int64_t lo, int64_t hi, double& np, double& nf) {
+        np = 0.0; nf = 0.0;
+        for (int64_t i = lo; i < hi; ++i) {
+            const ShellPairDev& d = P.h[g[i]];
+            np += (double)d.nprim1 * d.nprim2;
+            nf += (double)H.hb.nfunc[P.A[g[i]]] * H.hb.nfunc[P.B[g[i]]];
+        }
+    };
     for (int tb = 0; tb < kNumPairTypes; ++tb) {
         const int64_t nb = sb[tb + 1] - sb[tb];
         if (nb == 0) continue;
+        double npb, nfb;
+        sums(gb, sb[tb], sb[tb + 1], npb, nfb);
         if (mode == kModeDiagonal) {
+            double np2 = 0.0, nf2 = 0.0;
+            for (int64_t i = sb[tb]; i < sb[tb + 1]; ++i) {
+                const ShellPairDev& d = P.h[gb[i]];
+                const double x = (double)d.nprim1 * d.nprim2, y = (double)H.hb.nfunc[P.A[gb[i]]] * H.hb.nfunc[P.B[gb[i]]];
+                np2 += x * x; nf2 += y * y;
+            }
+            H.eri_stats[tb][tb][0] += (double)nb;
+            H.eri_stats[tb][tb][1] += np2;
+            H.eri_stats[tb][tb][2] += nf2;
             a.bra_ids = H.d_bra.p + sb[tb];
             a.ket_ids = a.bra_ids;
             a.nbra = nb;
@@ -425,6 +455,12 @@ static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<in
         for (int tk = 0; tk < kNumPairTypes; ++tk) {
             const int64_t nk = sk[tk + 1] - sk[tk];
             if (nk == 0) continue;
+            double npk, nfk;
+            sums(gk, sk[tk], sk[tk + 1], npk, nfk);
+            const int cb = std::max(tb, tk), ck = std::min(tb, tk);
+            H.eri_stats[cb][ck][0] += (double)nb * nk;
+            H.eri_stats[cb][ck][1] += npb * npk;
+            H.eri_stats[cb][ck][2] += nfb * nfk;
             a.bra_ids = H.d_bra.p + sb[tb];
             a.ket_ids = H.d_ket.p + sk[tk];
             a.nbra = nb;
@@ -724,6 +760,7 @@ static void step1(Handle& H)
                 dLB.ensure((size_t)nbatch * nchol);
                 CU(launch_gather_rows(Lst.p, ncand, dbrow.p, nbatch, nchol, dLB.p, nbatch, s));
                 gemm_nt(C.blas, ncand, nbatch, nchol, -1.0, Lst.p, ncand, dLB.p, nbatch, 1.0, dM.p, ncand);
+                H.gemm_flops[kGemmSubtractR] += 2.0 * ncand * nbatch * nchol;
             }
             T.stop();
             // -------- micro iterations (:1025-1064) on the batch block
@@ -764,6 +801,7 @@ static void step1(Handle& H)
                 dMp.ensure((size_t)ncand * npiv);
                 CU(launch_gather_cols(dM.p, ncand, dpiv.p, ncand, npiv, dMp.p, ncand, s));
                 gemm_nt(C.blas, ncand, npiv, npiv, 1.0, dMp.p, ncand, dLinv.p, npiv, 0.0, Lst.p + ncand * nchol, ncand);
+                H.gemm_flops[kGemmLnew] += 2.0 * ncand * npiv * npiv + (double)npiv * npiv * npiv / 3.0;
                 CU(launch_downdate(dD.p, Lst.p + ncand * nchol, ncand, ncand, npiv, s));
             }
             T.stop();
@@ -886,6 +924,7 @@ static void step2(Handle& H)
     CU(cudaStreamSynchronize(s));
     if (hinfo != 0) fail(GCI_ERR_NOT_SPD, "dtrtri failed: info=" + std::to_string(hinfo));
     T.stop();
+    H.gemm_flops[kGemmPotrf] += 2.0 * (double)N * N * N / 3.0;
     T.flush();
 }
 
@@ -928,6 +967,7 @@ static void materialize_rkpq(Handle& H)
         // real_abT: Rkpq(:,:,X) = Inv_L W^T
         H.timer.start(kInvLGemm);
         gemm_nt(C.blas, N, msd, N, 1.0, H.invl.p, N, W.p, msd, 0.0, H.rkpq.p + (size_t)N * msd * X, N);
+        H.gemm_flops[kGemmInvL] += 2.0 * N * N * (double)msd;
         H.timer.stop();
     }
     CU(cudaStreamSynchronize(s));
@@ -943,6 +983,7 @@ static void mo_two_gemms(Handle& H, int precision, const double* U, int64_t kc, 
     Context& C = ctx();
     const int64_t nao = H.hb.nao;
     const double one = 1.0, zero = 0.0;
+    H.gemm_flops[kGemmMo] += 2.0 * (double)nao * nao * kc * NA + 2.0 * (double)kc * NB * nao * NA;
     if (precision == GCI_PREC_FP64) {
         CB(cublasDgemm_64(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, nao * kc, NA, nao, &one, U, nao * kc, CAd, nao, &zero, W1,
                           nao * kc));
@@ -955,7 +996,8 @@ static void mo_two_gemms(Handle& H, int precision, const double* U, int64_t kc, 
 }
 
 static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int64_t a1, const double* CB_,
-                      int64_t ldcb, int64_t b0, int64_t b1, int64_t max_buffer_mb, int precision, double* rkab)
+                      int64_t ldcb, int64_t b0, int64_t b1, int64_t max_buffer_mb, int precision, double* rkab,
+                      bool device_io)
 {
     Context& C = ctx();
     cudaStream_t s = C.stream;
@@ -968,15 +1010,19 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
     if (precision != GCI_PREC_FP64 && precision != GCI_PREC_MIXED) fail(GCI_ERR_ARG, "invalid precision mode");
     if (N == 0) return;
     // MO coefficient blocks on the device
-    std::vector<double> ha((size_t)nao * NA), hbm((size_t)nao * NB);
-    for (int64_t a = 0; a < NA; ++a)
-        for (int64_t p = 0; p < nao; ++p) ha[p + nao * a] = CA[p + ldca * (a0 - 1 + a)];
-    for (int64_t a = 0; a < NB; ++a)
-        for (int64_t p = 0; p < nao; ++p) hbm[p + nao * a] = CB_[p + ldcb * (b0 - 1 + a)];
     DVec<double> dCA, dCB, dOut, U, W1;
-    dCA.upload(ha, s);
-    dCB.upload(hbm, s);
-    dOut.alloc((size_t)N * NA * NB);
+    dCA.alloc((size_t)nao * NA);
+    dCB.alloc((size_t)nao * NB);
+    const cudaMemcpyKind kind = device_io ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CU(cudaMemcpy2DAsync(dCA.p, sizeof(double) * nao, CA + ldca * (a0 - 1), sizeof(double) * ldca,
+                         sizeof(double) * nao, NA, kind, s));
+    CU(cudaMemcpy2DAsync(dCB.p, sizeof(double) * nao, CB_ + ldcb * (b0 - 1), sizeof(double) * ldcb,
+                         sizeof(double) * nao, NB, kind, s));
+    double* out_dev = rkab;
+    if (!device_io) {
+        dOut.alloc((size_t)N * NA * NB);
+        out_dev = dOut.p;
+    }
     // chunk of the fastest index so that U + W1 fit in the buffer budget
     const double budget = (max_buffer_mb > 0 ? (double)max_buffer_mb : 8192.0) * 1024.0 * 1024.0;
     int64_t kc = (int64_t)(budget / (8.0 * (double)(nao * nao + nao * NA)));
@@ -1010,7 +1056,7 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
             T.start(kMoGemm);
             CU(cudaMemsetAsync(U.p, 0, sizeof(double) * nao * nao * kk, s));
             CU(launch_unpack_rkpq(H.rkpq.p, N, dcol.p, dao.p, (int64_t)pqcol.size(), k0, kk, nao, U.p, s));
-            mo_two_gemms(H, precision, U.p, kk, dCA.p, NA, dCB.p, NB, W1.p, dOut.p + k0, N);
+            mo_two_gemms(H, precision, U.p, kk, dCA.p, NA, dCB.p, NB, W1.p, out_dev + k0, N);
             T.stop();
         }
     } else {
@@ -1050,10 +1096,11 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
         }
         T.start(kInvLGemm);
         const double one = 1.0, zero = 0.0;
-        CB(cublasDgemm_64(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, NA * NB, N, &one, H.invl.p, N, Vab.p, N, &zero, dOut.p, N));
+        CB(cublasDgemm_64(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, NA * NB, N, &one, H.invl.p, N, Vab.p, N, &zero, out_dev, N));
+        H.gemm_flops[kGemmInvL] += 2.0 * (double)N * N * NA * NB;
         T.stop();
     }
-    CU(cudaMemcpyAsync(rkab, dOut.p, sizeof(double) * N * NA * NB, cudaMemcpyDeviceToHost, s));
+    if (!device_io) CU(cudaMemcpyAsync(rkab, dOut.p, sizeof(double) * N * NA * NB, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     T.flush();
 }
@@ -1175,9 +1222,49 @@ int gci_rkab(gci_handle* h, const double* CA, int64_t ldca, int64_t a0, int64_t 
     if (!h || !CA || !CB || !rkab) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
     return guarded([&] {
         auto t0 = std::chrono::steady_clock::now();
-        rkab_impl(h->h, CA, ldca, a0, a1, CB, ldcb, b0, b1, max_buffer_mb, precision, rkab);
+        rkab_impl(h->h, CA, ldca, a0, a1, CB, ldcb, b0, b1, max_buffer_mb, precision, rkab, false);
         h->h.t_rkab = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     });
+}
+
+int gci_rkab_device(gci_handle* h, const double* CA, int64_t ldca, int64_t a0, int64_t a1, const double* CB,
+                    int64_t ldcb, int64_t b0, int64_t b1, int64_t max_buffer_mb, int precision, double* rkab)
+{
+    if (!h || !CA || !CB || !rkab) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        auto t0 = std::chrono::steady_clock::now();
+        rkab_impl(h->h, CA, ldca, a0, a1, CB, ldcb, b0, b1, max_buffer_mb, precision, rkab, true);
+        h->h.t_rkab = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    });
+}
+
+int gci_stats(const gci_handle* h, double* out, int n)
+{
+    if (!h || !out) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    const Handle& H = h->h;
+    std::vector<double> v(8 + 3 * kNumPairTypes * kNumPairTypes, 0.0);
+    for (int i = 0; i < kNumGemm; ++i) v[i] = H.gemm_flops[i];
+    for (int tb = 0; tb < kNumPairTypes; ++tb)
+        for (int tk = 0; tk < kNumPairTypes; ++tk)
+            for (int q = 0; q < 3; ++q) {
+                v[8 + 3 * (tb * kNumPairTypes + tk) + q] = H.eri_stats[tb][tk][q];
+                v[5 + q] += H.eri_stats[tb][tk][q];
+            }
+    for (int i = 0; i < n && i < (int)v.size(); ++i) out[i] = v[i];
+    return GCI_OK;
+}
+
+int gci_kernel_launches(int64_t* n)
+{
+    if (!n) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    *n = launches();
+    return GCI_OK;
+}
+
+int gci_get_stream(void** stream)
+{
+    if (!stream) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    return guarded([&] { *stream = (void*)ctx().stream; });
 }
 
 int gci_timings(const gci_handle* h, double* out, int n)

@@ -4,6 +4,10 @@
 
 namespace gci {
 
+// Number of kernels this library has launched (all launchers count themselves).
+void count_launch(int64_t n = 1);
+int64_t launches();
+
 cudaError_t eri_module_init();
 cudaError_t eri_launch(int tb, int tk, const EriArgs& args, cudaStream_t st);
 cudaError_t pair_records_launch(const ShellPairDev* pairs, int npairs, const double* xyz, const int* poff,

@@ -1,0 +1,90 @@
+"""Algorithmic work model of the Cholesky-ERI path.
+
+GEMM-type work is counted with the closed formulas of the stages (M - L L^T:
+2 NCand NBatch NChol_prev per macro iteration; pivot block: 2 N^3 / 3;
+Inv_L products: 2 N^2 x columns; AO->MO: 2 N NA NAO^2 + 2 N NA NB NAO).  ERI
+work is counted per canonical class (l_a >= l_b, l_c >= l_d, bra type >= ket
+type) from the arithmetic of the reference's W-matrix algorithm
+(auto2e_WMatrix_part*.f90: Boys, R_tuv recursion, ket and bra Hermite ->
+Cartesian transforms per primitive quartet; HRR and spherical transforms per
+contracted quartet), an FMA counted as two flops.  The counts of evaluated
+quartets come from the library (gci_stats) or the oracle (orc_stats).
+"""
+from __future__ import annotations
+
+from functools import lru_cache
+
+import numpy as np
+
+
+def ncart(l):
+    return (l + 1) * (l + 2) // 2
+
+
+def cart_off(l):
+    return l * (l + 1) * (l + 2) // 6
+
+
+def herm_n(n):
+    return (n + 1) * (n + 2) * (n + 3) // 6
+
+
+def carts(l):
+    return [(x, y, l - x - y) for x in range(l, -1, -1) for y in range(l - x, -1, -1)]
+
+
+def pair_types(lmax):
+    return [(hi, lo) for hi in range(lmax + 1) for lo in range(hi + 1)]
+
+
+@lru_cache(maxsize=None)
+def class_flops(la, lb, lc, ld, spher=True):
+    """(flops per primitive quartet, flops per contracted quartet) of one class."""
+    L1, L2 = la + lb, lc + ld
+    LT = L1 + L2
+    ebra = [c for l in range(la, L1 + 1) for c in carts(l)]
+    fket = [c for l in range(lc, L2 + 1) for c in carts(l)]
+    H1 = herm_n(L1)
+    boys = 30 + 3 * LT
+    pref = 25
+    rrec = 3 * sum(herm_n(n) for n in range(1, LT + 1))
+    s_build = 0
+    for fx, fy, fz in fket:
+        s_build += H1 * 2 * ((fx + 1) * (fy + 1) * (fz + 1) + (fy + 1) * (fz + 1) + (fz + 1))
+    w_acc = len(fket) * sum(2 * ((ex + 1) * (ey + 1) * (ez + 1) + (ey + 1) * (ez + 1) + (ez + 1))
+                            for ex, ey, ez in ebra)
+    prim = boys + pref + rrec + s_build + w_acc
+    nA, nB, nC, nD = ncart(la), ncart(lb), ncart(lc), ncart(ld)
+    nf = (lambda l: 2 * l + 1) if spher else ncart
+    fA, fB, fC, fD = nf(la), nf(lb), nf(lc), nf(ld)
+    NE = len(ebra)
+    hrr_k = NE * sum(4 * (dx + 1) * (dy + 1) * (dz + 1) for dx, dy, dz in carts(ld)) * nC
+    t_d = 2 * NE * nC * fD * nD
+    t_c = 2 * NE * fC * fD * nC
+    hrr_b = fC * fD * nA * sum(4 * (bx + 1) * (by + 1) * (bz + 1) for bx, by, bz in carts(lb))
+    t_b = 2 * nA * fB * fC * fD * nB
+    t_a = 2 * fA * fB * fC * fD * nA
+    epi = hrr_k + t_d + t_c + hrr_b + t_b + t_a
+    return prim, epi
+
+
+def eri_flops(stats: np.ndarray, ntypes: int, spher=True) -> float:
+    """ERI flops from a work-counter array (library or oracle layout)."""
+    types = pair_types({10: 3, 21: 5}[ntypes])
+    total = 0.0
+    for tb in range(ntypes):
+        for tk in range(ntypes):
+            q, pq, _ = stats[8 + 3 * (tb * ntypes + tk):8 + 3 * (tb * ntypes + tk) + 3]
+            if q == 0:
+                continue
+            (la, lb), (lc, ld) = types[tb], types[tk]
+            prim, epi = class_flops(la, lb, lc, ld, spher)
+            total += pq * prim + q * epi
+    return total
+
+
+def job_flops(stats: np.ndarray, ntypes: int, spher=True) -> dict:
+    gemm = float(np.sum(stats[:5]))
+    eri = eri_flops(stats, ntypes, spher)
+    return {"gemm": gemm, "eri": eri, "total": gemm + eri, "integrals": float(stats[7]),
+            "quartets": float(stats[5]), "prim_quartets": float(stats[6])}

@@ -111,6 +111,23 @@ int gci_rkab(gci_handle *h, const double *CA, int64_t ldca, int64_t a0, int64_t 
              const double *CB, int64_t ldcb, int64_t b0, int64_t b1, int64_t max_buffer_mb,
              int precision, double *rkab);
 
+/* gci_rkab with CA, CB and Rkab in device memory (no host copies); same layout. */
+int gci_rkab_device(gci_handle *h, const double *CA, int64_t ldca, int64_t a0, int64_t a1,
+                    const double *CB, int64_t ldcb, int64_t b0, int64_t b1, int64_t max_buffer_mb,
+                    int precision, double *rkab);
+
+/* Work done on this handle: [0..4] GEMM flops of M-LL^T, new vectors, potrf+trtri, Inv_L
+ * products, AO->MO; [5] shell quartets, [6] primitive quartets, [7] integrals evaluated;
+ * then per canonical class (bra type, ket type) of 10 x 10 pair types: quartets,
+ * primitive quartets, integrals.  Pair type of (l_hi, l_lo) = l_hi(l_hi+1)/2 + l_lo. */
+int gci_stats(const gci_handle *h, double *out, int n);
+
+/* Kernels of this library launched so far in the process (cuBLAS/cuSOLVER calls excluded). */
+int gci_kernel_launches(int64_t *n);
+
+/* The CUDA stream (cudaStream_t) every call of the library runs on. */
+int gci_get_stream(void **stream);
+
 /* Per-phase device times (seconds) of the last gci_rkpq/gci_rkab on this handle:
  * [0] Vdiag [1] step-1 ERI (time_2e) [2] M - L L^T (time_rTr) [3] pivots + vectors (time_rk)
  * [4] compress [5] V_JJ ERI [6] potrf+trtri [7] full-dim ERI [8] Inv_L GEMM [9] AO->MO GEMMs

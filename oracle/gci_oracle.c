@@ -627,6 +627,49 @@ L190:
 }
 
 /* ====================================================================== */
+/* Work counters (same layout as the library's gci_stats): [0..4] GEMM      */
+/* flops of M - L L^T, new vectors, potrf+trtri, Inv_L product, AO->MO;    */
+/* [5..7] shell quartets, primitive quartets, integrals; then per class    */
+/* (bra pair type, ket pair type) the same three counts.                   */
+/* ====================================================================== */
+#define NPT 21   /* pair types for l <= 5 */
+static double g_stats[8 + 3 * NPT * NPT];
+
+static inline int ptype(int la, int lb)
+{
+    int hi = la > lb ? la : lb, lo = la > lb ? lb : la;
+    return hi * (hi + 1) / 2 + lo;
+}
+
+void orc_stats_reset(void) { memset(g_stats, 0, sizeof(g_stats)); }
+
+void orc_stats(double *out, int n)
+{
+    for (int i = 0; i < n && i < (int)(sizeof(g_stats) / sizeof(double)); ++i) out[i] = g_stats[i];
+}
+
+static void count_quartet(const orc_basis *b, int A, int B, int C, int D)
+{
+    int t1 = ptype(b->L[A], b->L[B]), t2 = ptype(b->L[C], b->L[D]);
+    int hi = t1 > t2 ? t1 : t2, lo = t1 > t2 ? t2 : t1;
+    double nf = (double)nfunc(b, A) * nfunc(b, B) * nfunc(b, C) * nfunc(b, D);
+    double np = (double)b->nprim[A] * b->nprim[B] * b->nprim[C] * b->nprim[D];
+    double *c = g_stats + 8 + 3 * (hi * NPT + lo);
+#pragma omp atomic
+    c[0] += 1.0;
+#pragma omp atomic
+    c[1] += np;
+#pragma omp atomic
+    c[2] += nf;
+#pragma omp atomic
+    g_stats[5] += 1.0;
+#pragma omp atomic
+    g_stats[6] += np;
+#pragma omp atomic
+    g_stats[7] += nf;
+}
+
+/* ====================================================================== */
 /* Two-step Cholesky                                                        */
 /* ====================================================================== */
 
@@ -645,6 +688,7 @@ static void pq2p_ge_q(int64_t pq, int64_t n, int64_t *p, int64_t *q)
 /* ERI block of shells (A,B,C,D), a fastest; scratch is caller's */
 static void quartet_into(const orc_basis *b, int A, int B, int C, int D, double kappa, double *V)
 {
+    count_quartet(b, A, B, C, D);
     orc_eri_quartet(b, A, B, C, D, kappa, V);
 }
 
@@ -662,12 +706,12 @@ int orc_cholesky(const orc_basis *b, double tau, double kappa, int max_block_dim
                  int want_rkpq, int pivot_decode_storage, int nthreads, orc_chol *res)
 {
     return orc_cholesky_forced(b, tau, kappa, max_block_dim, want_rkpq, pivot_decode_storage, nthreads,
-                               NULL, 0, res);
+                               NULL, 0, 0, res);
 }
 
 int orc_cholesky_forced(const orc_basis *b, double tau, double kappa, int max_block_dim,
                         int want_rkpq, int pivot_decode_storage, int nthreads,
-                        const int64_t *forced_order, int64_t nforced, orc_chol *res)
+                        const int64_t *forced_order, int64_t nforced, int stage_limit, orc_chol *res)
 {
     memset(res, 0, sizeof(*res));
 #ifdef _OPENMP
@@ -811,6 +855,7 @@ int orc_cholesky_forced(const orc_basis *b, double tau, double kappa, int max_bl
         res->max_subset_dim = mx;
     }
 
+    if (stage_limit == 1) { free(D); return 1; }
     /* ---------------- chol2_Pivots, Step1.f90:884-1103 ---------------- */
     int64_t maxnchol = (int64_t)ceil(nao * 15.0);
     if (maxnchol > npq) maxnchol = npq;
@@ -946,6 +991,7 @@ int orc_cholesky_forced(const orc_basis *b, double tau, double kappa, int max_bl
                 int64_t s = bmap[k];
                 for (int i = 0; i < res->shellpairdim[s]; ++i) brow[colloc[k] + i] = compr[s] + i;
             }
+            g_stats[0] += 2.0 * ncand * nbatch * nchol;
 #pragma omp parallel for schedule(static)
             for (int64_t q = 0; q < nbatch; ++q) {
                 double *Mc = M + (size_t)ncand * q;
@@ -988,6 +1034,7 @@ int orc_cholesky_forced(const orc_basis *b, double tau, double kappa, int max_bl
             /* chol2_Lj :859-881 */
             double *Lj = Lm + (size_t)ncand * (j - 1);
             memcpy(Lj, M + (size_t)ncand * maxlocbatch, sizeof(double) * ncand);
+            g_stats[1] += 2.0 * ncand * (j - 1);
             if (j > 1) {
                 double *Tq = (double *)malloc(sizeof(double) * (j - 1));
                 for (int64_t i = 0; i < j - 1; ++i) Tq[i] = Lm[(size_t)ncand * i + maxloc];
@@ -1013,6 +1060,7 @@ int orc_cholesky_forced(const orc_basis *b, double tau, double kappa, int max_bl
         for (int64_t p = 0; p < ncand; ++p) if (D[p] > dmax) dmax = D[p];
         if (dmax <= tau) { converged = 1; macro_go = 0; }
         if (nchol == maxnchol || nbatch == 0) macro_go = 0;
+        if (stage_limit == 2) macro_go = 0;
     }
     res->n_macro = nmacro;
     res->nvecs = nchol;
@@ -1020,6 +1068,7 @@ int orc_cholesky_forced(const orc_basis *b, double tau, double kappa, int max_bl
     res->dmax_final = dmax;
     free(bmap); free(colloc); free(sortv); free(sorti); free(candmap); free(compr);
     free(Lst); free(D);
+    if (stage_limit == 2) { res->nvecs = nchol; return 2; }
     if (nchol == maxnchol && !converged) return -4;
 
     /* ---------------- chol2_PivotShellPairs, Step2.f90:469-534 ---------------- */
@@ -1080,6 +1129,7 @@ int orc_cholesky_forced(const orc_basis *b, double tau, double kappa, int max_bl
                     Vq[res->pivorbpairs[pq0 + pq] + (size_t)Na * Nb * res->pivorbpairs[rs0 + rs]];
         free(Vq);
     }
+    g_stats[2] += 2.0 * (double)N * N * N / 3.0;
     /* real_Cholesky (dpotrf "L", upper zeroed) real_linalg.f90:39-58 */
     for (int64_t jj = 0; jj < N; ++jj) {
         double s = V[jj + N * jj];
@@ -1144,6 +1194,7 @@ int orc_cholesky_forced(const orc_basis *b, double tau, double kappa, int max_bl
                     free(Vq);
                 }
             /* real_abT: Rkpq(:,:,X) = InvL * W^T */
+            g_stats[3] += 2.0 * (double)N * N * msd;
             double *R = res->rkpq + (size_t)N * msd * X;
             const double *Inv = res->inv_l;
 #pragma omp parallel for schedule(static)
@@ -1212,6 +1263,7 @@ int orc_mo_transf(const orc_chol *c, const orc_basis *b, const int *shell_loc,
                 }
         }
     }
+    g_stats[4] += 2.0 * (double)N * NA * nao * nao + 2.0 * (double)N * NA * NB * nao;
     /* Step 2: Rab(:, a, b) += sum_p W(:, a, p) CB(p, b) */
 #pragma omp parallel for schedule(static)
     for (int64_t bb = 0; bb < NB; ++bb)

@@ -80,7 +80,11 @@ int  orc_cholesky(const orc_basis *b, double tau, double kappa, int max_block_di
 /* the same with the step-1 pivot sequence given (FULL indices, 0-based): step 2 only */
 int  orc_cholesky_forced(const orc_basis *b, double tau, double kappa, int max_block_dim,
                          int want_rkpq, int pivot_decode_storage, int nthreads,
-                         const int64_t *forced_order, int64_t nforced, orc_chol *res);
+                         const int64_t *forced_order, int64_t nforced, int stage_limit, orc_chol *res);
+/* stage_limit: 0 full run, 1 stop after the diagonal and the Schwarz screen (returns 1),
+ * 2 stop after the first macro iteration of the pivot search (returns 2). */
+void orc_stats_reset(void);
+void orc_stats(double *out, int n);
 void orc_chol_free(orc_chol *res);
 
 /* AO->MO (Cholesky_Gammcor.f90:143-332): CA, CB are NAO x (ncol) column-major

@@ -71,7 +71,9 @@ def lib():
         L.orc_cholesky.argtypes = [C.POINTER(_Basis), C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.POINTER(_Chol)]
         L.orc_cholesky_forced.argtypes = [C.POINTER(_Basis), C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
-                                          C.c_int, _pl, _i64, C.POINTER(_Chol)]
+                                          C.c_int, _pl, _i64, C.c_int, C.POINTER(_Chol)]
+        L.orc_stats.argtypes = [_pd, C.c_int]
+        L.orc_stats_reset.argtypes = []
         L.orc_chol_free.argtypes = [C.POINTER(_Chol)]
         L.orc_mo_transf.argtypes = [C.POINTER(_Chol), C.POINTER(_Basis), _pi, _pd, _i64, _i64, _i64, _pd, _i64,
                                     _i64, _i64, C.c_int, _pd]
@@ -249,7 +251,7 @@ def cholesky(b: OracleBasis, tau: float, kappa: float = 0.0, want_rkpq: bool = T
     else:
         fo = np.ascontiguousarray(forced_order, dtype=np.int64)
         rc = lib().orc_cholesky_forced(C.byref(bs), tau, kappa, max_block_dim, int(want_rkpq), int(decode_storage),
-                                       nthreads, _p(fo, _pl), fo.size, C.byref(res))
+                                       nthreads, _p(fo, _pl), fo.size, 0, C.byref(res))
     if rc != 0:
         lib().orc_chol_free(C.byref(res))
         raise RuntimeError(f"orc_cholesky failed ({rc})")
@@ -274,6 +276,29 @@ def cholesky(b: OracleBasis, tau: float, kappa: float = 0.0, want_rkpq: bool = T
         rkpq=(_arr(res.rkpq, n * msd * ns, np.float64).reshape(n, msd, ns, order="F") if res.rkpq else None),
         _raw=res, _basis=b)
     return out
+
+
+def stats_reset() -> None:
+    lib().orc_stats_reset()
+
+
+def stats() -> np.ndarray:
+    """Work counters: [0..4] GEMM flops, [5..7] quartets / primitive quartets / integrals, then per
+    class (bra pair type, ket pair type) over 21 x 21 pair types (l <= 5)."""
+    out = np.zeros(8 + 3 * 21 * 21)
+    lib().orc_stats(_p(out), out.size)
+    return out
+
+
+def cholesky_stage(b: OracleBasis, tau: float, stage: int, nthreads: int = 0) -> int:
+    """Run the pipeline up to a stage (1: diagonal + screen, 2: first macro iteration)."""
+    res = _Chol()
+    bs = b.cstruct()
+    rc = lib().orc_cholesky_forced(C.byref(bs), tau, 0.0, 4000, 0, 0, nthreads, None, 0, stage, C.byref(res))
+    lib().orc_chol_free(C.byref(res))
+    if rc < 0:
+        raise RuntimeError(f"orc_cholesky stage failed ({rc})")
+    return rc
 
 
 def mo_transf(ch: OracleCholesky, b: OracleBasis, CA, a0, a1, CB, b0, b1, nthreads=0) -> np.ndarray:
