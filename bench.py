@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--buffer-mb", type=int, default=16384)
+    ap.add_argument("--decode-storage", action="store_true",
+                    help="decode diagonal-shell-pair pivots in storage order (GCI_FLAG_PIVOT_DECODE_STORAGE)")
     return ap.parse_args()
 
 
@@ -138,7 +140,7 @@ def cpu_baseline_c1():
     O.mo_transf(ch, b, Cm, 0, nocc - 1, Cm, nocc, nocc + nvirt - 1)
     dt = time.perf_counter() - t0
     O.free(ch)
-    f = flops.job_flops(O.stats(), 21)
+    f = flops.job_flops(O.stats(), "oracle")
     return {"value": f["total"] / dt / 1e9, "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port",
             "sample": f"full c1 job (10 atoms, NAO={b.nao}, {ch.nvecs} vectors, MO 20x60) in {dt:.1f} s "
                       f"on the oracle (FP64 C restatement of the reference, OpenMP)",
@@ -167,7 +169,7 @@ def run_reference(args, rank):
         O.mo_transf(ch, ob, Cm, 0, nocc - 1, Cm, nocc, nocc + nvirt - 1)
         dt = time.perf_counter() - t0
         O.free(ch)
-        return dt, flops.job_flops(O.stats(), 21)["total"]
+        return dt, flops.job_flops(O.stats(), "oracle")["total"]
 
     for _ in range(max(0, min(args.warmup, 1))):
         step()
@@ -234,7 +236,8 @@ def main():
 
     def job():
         h = C.c_void_p()
-        _capi.check(L.gci_rkpq(C.byref(bstruct), cg.CHOL_ACCURACY_TIGHT, 0.0, 0, C.byref(h)))
+        flags = _capi.GCI_FLAG_PIVOT_DECODE_STORAGE if args.decode_storage else 0
+        _capi.check(L.gci_rkpq(C.byref(bstruct), cg.CHOL_ACCURACY_TIGHT, 0.0, flags, C.byref(h)))
         nv = C.c_int64()
         _capi.check(L.gci_query(h, C.byref(nv), None, None, None, None, None))
         if state["rkab"] is None or state["nvecs"] != nv.value:
@@ -242,7 +245,7 @@ def main():
             state["nvecs"] = nv.value
         _capi.check(L.gci_rkab_device(h, C.c_void_p(c_dev.data_ptr()), nao, a0, a1, C.c_void_p(c_dev.data_ptr()),
                                       nao, b0, b1, args.buffer_mb, prec, C.c_void_p(state["rkab"].data_ptr())))
-        st = np.zeros(8 + 300)
+        st = np.zeros(8 + 400)
         _capi.check(L.gci_stats(h, _capi.ptr(st), st.size))
         tm = np.zeros(13)
         _capi.check(L.gci_timings(h, _capi.ptr(tm), 13))
@@ -273,7 +276,7 @@ def main():
     if world > 1:
         dist.all_reduce(t_tensor, op=dist.ReduceOp.MAX)
     t_max = float(t_tensor.item())
-    fl = flops.job_flops(stats[-1], 10)
+    fl = flops.job_flops(stats[-1], "lib")
     flops_step = fl["total"]
     value = flops_step * args.steps * world / t_max / 1e9
 
@@ -287,7 +290,8 @@ def main():
         barrier()
         e0.record(lib_stream)
         for _ in range(args.e2e_steps):
-            res = cg.chol_gammcor_Rkpq(tb, cg.CHOL_ACCURACY_TIGHT, materialize=False)
+            res = cg.chol_gammcor_Rkpq(tb, cg.CHOL_ACCURACY_TIGHT, materialize=False,
+                                       decode_storage=args.decode_storage)
             _capi.check(L.gci_rkab(res.handle.ptr, _capi.ptr(pin_c.numpy()), nao, a0, a1, _capi.ptr(pin_c.numpy()),
                                    nao, b0, b1, args.buffer_mb, prec, _capi.ptr(pin_out.numpy())))
             checksum = float(pin_out[:16].sum())
@@ -314,7 +318,7 @@ def main():
     eri_t = tm[0] + tm[1] + tm[5] + tm[7]
     gemm_t = tm[2] + tm[8] + tm[9]
     peak64 = measured_fp64_peak(torch)
-    eri_rate = fl["eri"] / eri_t / 1e12 if eri_t > 0 else 0.0
+    eri_rate = fl["eri_executed"] / eri_t / 1e12 if eri_t > 0 else 0.0
     roof = {"bound": "fp64", "kernel": "k_eri_class (all ERI stages)", "achieved": eri_rate, "peak": peak64,
             "unit": "TFLOP/s", "frac": eri_rate / peak64 if peak64 else None, "traffic": None,
             "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64; MEASURED_PEAKS.json has no FP64 figure)",
@@ -330,6 +334,9 @@ def main():
                        "precision": args.precision, "nvecs": state["nvecs"], "parallelism": f"replicas x{world}",
                        "l2": "working set (Rkab, ERI buffers) far above L2 (126 MB)"},
             "wall_s_per_step": t_max / args.steps, "gflop_per_step": flops_step / 1e9,
+            "gflop_executed_per_step": fl["executed"] / 1e9,
+            "value_definition": "reference-algorithm work (GEMM formulas + W-matrix ERI arithmetic over every "
+                                "primitive quartet, flops.py) per second of device time",
             "eri_per_s": fl["integrals"] * args.steps * world / t_max, "phases_s": phases,
             "gpu_launches": int(n1.value - n0.value), "roofline": roof, "e2e": e2e,
             "clocks": clk.summary(), "cpu_baseline": cpu}

@@ -168,8 +168,8 @@ k_eri_class(const EriArgs a)
         const ShellPairDev pk = a.pairs[ck];
         const double* __restrict__ rb = a.pp + pb.rec_off;
         const double* __restrict__ rk = a.pp + pk.rec_off;
-        const int nbp = pb.nprim1 * pb.nprim2;
-        const int nkp = pk.nprim1 * pk.nprim2;
+        const int nbp = pb.npp;
+        const int nkp = pk.npp;
 
         for (int w = lane; w < S::NE * S::NF; w += TW) WW[w] = 0.0;
         // lane -> ket Hermite index g and the R indices it reads

@@ -12,18 +12,19 @@ namespace gci {
 __global__ void k_pair_records(const ShellPairDev* __restrict__ pairs, int npairs,
                                const double* __restrict__ xyz, const int* __restrict__ poff,
                                const double* __restrict__ exps, const double* __restrict__ coefs,
-                               double* __restrict__ pp)
+                               const int* __restrict__ plist, double* __restrict__ pp)
 {
     for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
         const ShellPairDev sp = pairs[p];
         const int L1 = sp.l1 + sp.l2;
         const int rs = pp_record(L1);
-        const int n = sp.nprim1 * sp.nprim2;
+        const int n = sp.npp;
         const double ax = xyz[3 * sp.s1], ay = xyz[3 * sp.s1 + 1], az = xyz[3 * sp.s1 + 2];
         const double bx = xyz[3 * sp.s2], by = xyz[3 * sp.s2 + 1], bz = xyz[3 * sp.s2 + 2];
         const double r2 = (ax - bx) * (ax - bx) + (ay - by) * (ay - by) + (az - bz) * (az - bz);
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int ga = i % sp.nprim1, gb = i / sp.nprim1;
+            const int code = plist[sp.list_off + i];
+            const int ga = code & 0xff, gb = code >> 8;
             const double ea = exps[poff[sp.s1] + ga], eb = exps[poff[sp.s2] + gb];
             const double ca = coefs[poff[sp.s1] + ga], cb = coefs[poff[sp.s2] + gb];
             const double P = ea + eb;
@@ -93,11 +94,12 @@ cudaError_t eri_launch(int tb, int tk, const EriArgs& args, cudaStream_t st)
 }
 
 cudaError_t pair_records_launch(const ShellPairDev* pairs, int npairs, const double* xyz, const int* poff,
-                                const double* exps, const double* coefs, double* pp, cudaStream_t st)
+                                const double* exps, const double* coefs, const int* plist, double* pp,
+                                cudaStream_t st)
 {
     if (npairs <= 0) return cudaSuccess;
     int blocks = npairs < 148 * 64 ? npairs : 148 * 64;
-    k_pair_records<<<blocks, 64, 0, st>>>(pairs, npairs, xyz, poff, exps, coefs, pp);
+    k_pair_records<<<blocks, 64, 0, st>>>(pairs, npairs, xyz, poff, exps, coefs, plist, pp);
     count_launch();
     return cudaGetLastError();
 }

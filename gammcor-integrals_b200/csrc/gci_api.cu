@@ -260,6 +260,7 @@ struct PairTable {
     std::vector<ShellPairDev> h;
     DVec<ShellPairDev> d;
     DVec<double> pp;
+    DVec<int> plist;
 };
 
 static int64_t pair_local(int a, int b, int Na, bool same)
@@ -328,10 +329,17 @@ struct Handle {
     double t_rkpq = 0.0, t_rkab = 0.0;
     // work counters: GEMM flops per phase and ERI work per canonical class
     double gemm_flops[kNumGemm] = {0};
-    double eri_stats[kNumPairTypes][kNumPairTypes][3] = {};   // shell quartets, primitive quartets, integrals
+    double eri_stats[kNumPairTypes][kNumPairTypes][4] = {};   // quartets, prim quartets evaluated, integrals, prim quartets unscreened
     // scratch reused across ERI launches
     DVec<int> d_bra, d_ket;
 };
+
+// Primitive pairs whose weight |c_a c_b| K_ab (pi/P)^{3/2} (1+|PA|)^la (1+|PB|)^lb is
+// below kPrimRel of the largest in the shell pair, or below kPrimAbs, are not
+// stored: their share of any integral is below the FP64 rounding level.  The
+// reference evaluates every primitive quartet; the difference is < 1e-15 relative.
+static constexpr double kPrimRel = 1.0e-17;
+static constexpr double kPrimAbs = 1.0e-22;
 
 static void setup_pairs(Handle& H)
 {
@@ -342,6 +350,11 @@ static void setup_pairs(Handle& H)
     P.n = (int64_t)nsh * (nsh + 1) / 2;
     P.A.resize(P.n); P.B.resize(P.n); P.type.resize(P.n); P.dim.resize(P.n); P.nab.resize(P.n);
     P.vdloc.resize(P.n); P.h.resize(P.n);
+    std::vector<int> plist;
+    std::vector<double> w;
+    std::vector<double> minexp(nsh, 1e300);
+    for (int s = 0; s < nsh; ++s)
+        for (int i = 0; i < b.nprim[s]; ++i) minexp[s] = std::min(minexp[s], b.exps[b.poff[s] + i]);
     int64_t sp = 0, loc = 0, rec = 0;
     for (int B = 0; B < nsh; ++B)
         for (int A = B; A < nsh; ++A) {
@@ -352,7 +365,11 @@ static void setup_pairs(Handle& H)
             P.vdloc[sp] = loc;
             loc += P.dim[sp];
             ShellPairDev d{};
-            const bool sw = b.L[A] < b.L[B];
+            // canonical orientation: higher l first (as the reference's frontends);
+            // for equal l the tighter shell (larger smallest exponent) is the origin of
+            // the horizontal recurrence, which keeps its cancellation bounded
+            bool sw = b.L[A] < b.L[B];
+            if (b.L[A] == b.L[B] && A != B) sw = minexp[A] < minexp[B];
             d.s1 = sw ? B : A;
             d.s2 = sw ? A : B;
             d.swap = sw ? 1 : 0;
@@ -360,8 +377,38 @@ static void setup_pairs(Handle& H)
             d.l2 = b.L[d.s2];
             d.nprim1 = b.nprim[d.s1];
             d.nprim2 = b.nprim[d.s2];
+            const double* ra = &b.xyz[3 * d.s1];
+            const double* rb = &b.xyz[3 * d.s2];
+            const double r2 = (ra[0] - rb[0]) * (ra[0] - rb[0]) + (ra[1] - rb[1]) * (ra[1] - rb[1]) +
+                              (ra[2] - rb[2]) * (ra[2] - rb[2]);
+            const double r = std::sqrt(r2);
+            w.assign((size_t)d.nprim1 * d.nprim2, 0.0);
+            double wmax = 0.0;
+            for (int gb = 0; gb < d.nprim2; ++gb)
+                for (int ga = 0; ga < d.nprim1; ++ga) {
+                    const double ea = b.exps[b.poff[d.s1] + ga], eb = b.exps[b.poff[d.s2] + gb];
+                    const double ca = b.coefs[b.poff[d.s1] + ga], cb = b.coefs[b.poff[d.s2] + gb];
+                    const double p = ea + eb;
+                    const double kab = std::exp(-ea * eb / p * r2);
+                    const double pa = eb / p * r, pbd = ea / p * r;   // |P - A|, |P - B|
+                    const double v = std::fabs(ca * cb) * kab * std::pow(kPi / p, 1.5) *
+                                     std::pow(1.0 + pa, d.l1) * std::pow(1.0 + pbd, d.l2);
+                    w[ga + (size_t)d.nprim1 * gb] = v;
+                    wmax = std::max(wmax, v);
+                }
+            d.list_off = (int64_t)plist.size();
+            int kept = 0;
+            for (int gb = 0; gb < d.nprim2; ++gb)
+                for (int ga = 0; ga < d.nprim1; ++ga) {
+                    const double v = w[ga + (size_t)d.nprim1 * gb];
+                    if (v >= kPrimAbs && v >= kPrimRel * wmax) {
+                        plist.push_back(ga | (gb << 8));
+                        ++kept;
+                    }
+                }
+            d.npp = kept;
             d.rec_off = rec;
-            rec += (int64_t)d.nprim1 * d.nprim2 * pp_record(d.l1 + d.l2);
+            rec += (int64_t)kept * pp_record(d.l1 + d.l2);
             P.type[sp] = pair_type(d.l1, d.l2);
             P.h[sp] = d;
             ++sp;
@@ -376,8 +423,10 @@ static void setup_pairs(Handle& H)
     D.loc.upload(b.loc, C.stream);
     D.toff.upload(b.toff, C.stream);
     P.d.upload(P.h, C.stream);
+    if (plist.empty()) plist.push_back(0);
+    P.plist.upload(plist, C.stream);
     P.pp.alloc(rec > 0 ? rec : 1);
-    CU(pair_records_launch(P.d.p, (int)P.n, D.xyz.p, D.poff.p, D.exps.p, D.coefs.p, P.pp.p, C.stream));
+    CU(pair_records_launch(P.d.p, (int)P.n, D.xyz.p, D.poff.p, D.exps.p, D.coefs.p, P.plist.p, P.pp.p, C.stream));
 }
 
 static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<int>& ket, int mode, PairMap* rows,
@@ -421,29 +470,32 @@ static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<in
     a.kappa = H.kappa;
     a.boys = C.boys.p;
     a.err = C.err.p;
-    auto sums = [&](const std::vector<int>& g, int64_t lo, int64_t hi, double& np, double& nf) {
-        np = 0.0; nf = 0.0;
+    auto sums = [&](const std::vector<int>& g, int64_t lo, int64_t hi, double& np, double& nf, double& nu) {
+        np = 0.0; nf = 0.0; nu = 0.0;
         for (int64_t i = lo; i < hi; ++i) {
             const ShellPairDev& d = P.h[g[i]];
-            np += (double)d.nprim1 * d.nprim2;
+            np += (double)d.npp;
+            nu += (double)d.nprim1 * d.nprim2;
             nf += (double)H.hb.nfunc[P.A[g[i]]] * H.hb.nfunc[P.B[g[i]]];
         }
     };
     for (int tb = 0; tb < kNumPairTypes; ++tb) {
         const int64_t nb = sb[tb + 1] - sb[tb];
         if (nb == 0) continue;
-        double npb, nfb;
-        sums(gb, sb[tb], sb[tb + 1], npb, nfb);
+        double npb, nfb, nub;
+        sums(gb, sb[tb], sb[tb + 1], npb, nfb, nub);
         if (mode == kModeDiagonal) {
-            double np2 = 0.0, nf2 = 0.0;
+            double np2 = 0.0, nf2 = 0.0, nu2 = 0.0;
             for (int64_t i = sb[tb]; i < sb[tb + 1]; ++i) {
                 const ShellPairDev& d = P.h[gb[i]];
-                const double x = (double)d.nprim1 * d.nprim2, y = (double)H.hb.nfunc[P.A[gb[i]]] * H.hb.nfunc[P.B[gb[i]]];
-                np2 += x * x; nf2 += y * y;
+                const double x = (double)d.npp, y = (double)H.hb.nfunc[P.A[gb[i]]] * H.hb.nfunc[P.B[gb[i]]];
+                const double u = (double)d.nprim1 * d.nprim2;
+                np2 += x * x; nf2 += y * y; nu2 += u * u;
             }
             H.eri_stats[tb][tb][0] += (double)nb;
             H.eri_stats[tb][tb][1] += np2;
             H.eri_stats[tb][tb][2] += nf2;
+            H.eri_stats[tb][tb][3] += nu2;
             a.bra_ids = H.d_bra.p + sb[tb];
             a.ket_ids = a.bra_ids;
             a.nbra = nb;
@@ -455,12 +507,13 @@ static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<in
         for (int tk = 0; tk < kNumPairTypes; ++tk) {
             const int64_t nk = sk[tk + 1] - sk[tk];
             if (nk == 0) continue;
-            double npk, nfk;
-            sums(gk, sk[tk], sk[tk + 1], npk, nfk);
+            double npk, nfk, nuk;
+            sums(gk, sk[tk], sk[tk + 1], npk, nfk, nuk);
             const int cb = std::max(tb, tk), ck = std::min(tb, tk);
             H.eri_stats[cb][ck][0] += (double)nb * nk;
             H.eri_stats[cb][ck][1] += npb * npk;
             H.eri_stats[cb][ck][2] += nfb * nfk;
+            H.eri_stats[cb][ck][3] += nub * nuk;
             a.bra_ids = H.d_bra.p + sb[tb];
             a.ket_ids = H.d_ket.p + sk[tk];
             a.nbra = nb;
@@ -1242,13 +1295,13 @@ int gci_stats(const gci_handle* h, double* out, int n)
 {
     if (!h || !out) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
     const Handle& H = h->h;
-    std::vector<double> v(8 + 3 * kNumPairTypes * kNumPairTypes, 0.0);
+    std::vector<double> v(8 + 4 * kNumPairTypes * kNumPairTypes, 0.0);
     for (int i = 0; i < kNumGemm; ++i) v[i] = H.gemm_flops[i];
     for (int tb = 0; tb < kNumPairTypes; ++tb)
         for (int tk = 0; tk < kNumPairTypes; ++tk)
-            for (int q = 0; q < 3; ++q) {
-                v[8 + 3 * (tb * kNumPairTypes + tk) + q] = H.eri_stats[tb][tk][q];
-                v[5 + q] += H.eri_stats[tb][tk][q];
+            for (int q = 0; q < 4; ++q) {
+                v[8 + 4 * (tb * kNumPairTypes + tk) + q] = H.eri_stats[tb][tk][q];
+                if (q < 3) v[5 + q] += H.eri_stats[tb][tk][q];
             }
     for (int i = 0; i < n && i < (int)v.size(); ++i) out[i] = v[i];
     return GCI_OK;

@@ -52,7 +52,9 @@ struct ShellPairDev {
     int swap;            // 1 if s1 is the second shell of the stored pair (A >= B index order)
     int nprim1, nprim2;
     int l1, l2;          // angular momenta of s1, s2
+    int npp;             // primitive pairs kept after screening (records stored)
     int64_t rec_off;     // offset (doubles) of the first primitive-pair record
+    int64_t list_off;    // offset of the kept (ga | gb << 8) list
 };
 
 struct EriArgs {

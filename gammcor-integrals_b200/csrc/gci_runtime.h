@@ -11,7 +11,8 @@ int64_t launches();
 cudaError_t eri_module_init();
 cudaError_t eri_launch(int tb, int tk, const EriArgs& args, cudaStream_t st);
 cudaError_t pair_records_launch(const ShellPairDev* pairs, int npairs, const double* xyz, const int* poff,
-                                const double* exps, const double* coefs, double* pp, cudaStream_t st);
+                                const double* exps, const double* coefs, const int* plist, double* pp,
+                                cudaStream_t st);
 cudaError_t boys_eval_launch(int m, int64_t n, const double* x, const double* table, double* out, cudaStream_t st);
 
 cudaError_t launch_segmax(const double* D, const int64_t* loc, const int* dim, int64_t n, double* out, cudaStream_t s);

@@ -68,13 +68,24 @@ def class_flops(la, lb, lc, ld, spher=True):
     return prim, epi
 
 
-def eri_flops(stats: np.ndarray, ntypes: int, spher=True) -> float:
-    """ERI flops from a work-counter array (library or oracle layout)."""
+# Counter layouts: the library (gci_stats) keeps 4 counters per class over
+# 10 pair types -- quartets, primitive quartets evaluated, integrals, primitive
+# quartets before the primitive-pair screen; the oracle (orc_stats) keeps 3
+# per class over 21 pair types and evaluates every primitive quartet.
+LAYOUTS = {"lib": (10, 4), "oracle": (21, 3)}
+
+
+def eri_flops(stats: np.ndarray, layout: str, spher=True, unscreened=False) -> float:
+    """ERI flops from a work-counter array.  ``unscreened`` counts the primitive
+    quartets the reference algorithm evaluates (no primitive screening)."""
+    ntypes, nc = LAYOUTS[layout]
     types = pair_types({10: 3, 21: 5}[ntypes])
+    col = 3 if (unscreened and nc == 4) else 1
     total = 0.0
     for tb in range(ntypes):
         for tk in range(ntypes):
-            q, pq, _ = stats[8 + 3 * (tb * ntypes + tk):8 + 3 * (tb * ntypes + tk) + 3]
+            base = 8 + nc * (tb * ntypes + tk)
+            q, pq = stats[base], stats[base + col]
             if q == 0:
                 continue
             (la, lb), (lc, ld) = types[tb], types[tk]
@@ -83,8 +94,12 @@ def eri_flops(stats: np.ndarray, ntypes: int, spher=True) -> float:
     return total
 
 
-def job_flops(stats: np.ndarray, ntypes: int, spher=True) -> dict:
+def job_flops(stats: np.ndarray, layout: str, spher=True) -> dict:
+    """GEMM + ERI work of a job: ``total`` in the reference algorithm's terms
+    (every primitive quartet), ``executed`` what was actually evaluated."""
     gemm = float(np.sum(stats[:5]))
-    eri = eri_flops(stats, ntypes, spher)
-    return {"gemm": gemm, "eri": eri, "total": gemm + eri, "integrals": float(stats[7]),
-            "quartets": float(stats[5]), "prim_quartets": float(stats[6])}
+    eri_ref = eri_flops(stats, layout, spher, unscreened=True)
+    eri_run = eri_flops(stats, layout, spher, unscreened=False)
+    return {"gemm": gemm, "eri": eri_ref, "eri_executed": eri_run, "total": gemm + eri_ref,
+            "executed": gemm + eri_run, "integrals": float(stats[7]), "quartets": float(stats[5]),
+            "prim_quartets": float(stats[6])}

@@ -119,7 +119,8 @@ int gci_rkab_device(gci_handle *h, const double *CA, int64_t ldca, int64_t a0, i
 /* Work done on this handle: [0..4] GEMM flops of M-LL^T, new vectors, potrf+trtri, Inv_L
  * products, AO->MO; [5] shell quartets, [6] primitive quartets, [7] integrals evaluated;
  * then per canonical class (bra type, ket type) of 10 x 10 pair types: quartets,
- * primitive quartets, integrals.  Pair type of (l_hi, l_lo) = l_hi(l_hi+1)/2 + l_lo. */
+ * primitive quartets evaluated, integrals, primitive quartets before the primitive-pair
+ * screen.  Pair type of (l_hi, l_lo) = l_hi(l_hi+1)/2 + l_lo. */
 int gci_stats(const gci_handle *h, double *out, int n);
 
 /* Kernels of this library launched so far in the process (cuBLAS/cuSOLVER calls excluded). */

@@ -535,6 +535,32 @@ static inline int nfunc(const orc_basis *b, int s)
 /* One normalised (spherical or Cartesian) shell quartet, V(a,b,c,d) with a
  * fastest -- the layout a caller of Auto2eERI obtains by passing the shells
  * in the order (D,C,B,A) (auto2e.f90:1-34, TwoStepCholesky_Step1.f90:812-838). */
+/* Canonical orientation of a class, as the reference's frontends arrange it
+ * (e.g. auto2e_frontend_1_2_1_2, auto2e_eri_dpdp.f90:334-351): the higher
+ * angular momentum first within each pair, and the bra pair not below the
+ * ket pair in the (l_hi, l_lo) order.  The HRR's rounding depends on the
+ * orientation, so the oracle evaluates the same canonical class. */
+static inline int pair_rank(int lhi, int llo) { return lhi * (lhi + 1) / 2 + llo; }
+
+static double min_exponent(const orc_basis *b, int s)
+{
+    double m = 1e300;
+    for (int i = 0; i < b->nprim[s]; ++i) m = fmin(m, b->exps[b->prim_off[s] + i]);
+    return m;
+}
+
+/* 1 if shell x stays first in the pair (x, y).  Higher l first, as in the
+ * reference.  For equal l the reference keeps the given order; here the
+ * shell with the larger smallest exponent goes first, because the HRR
+ * (a,b| = sum C(b,k) (A-B)^{b-k} (a+k,0| loses up to ~6 digits when A is the
+ * diffuse shell of a distant pair (the product centre P is then far from A).
+ * Ties keep the given order. */
+static int orient_first(const orc_basis *b, int x, int y)
+{
+    if (b->L[x] != b->L[y]) return b->L[x] > b->L[y];
+    return min_exponent(b, x) >= min_exponent(b, y);
+}
+
 int orc_eri_quartet(const orc_basis *b, int A, int B, int C, int D, double kappa, double *out)
 {
     int sh[4] = {A, B, C, D};
@@ -547,16 +573,39 @@ int orc_eri_quartet(const orc_basis *b, int A, int B, int C, int D, double kappa
         nf[i] = nfunc(b, sh[i]);
         T[i] = b->T + b->T_off[sh[i]];
     }
-    double *G = (double *)malloc(sizeof(double) * n[0] * n[1] * n[2] * n[3]);
-    cart_quartet(l[0], l[1], l[2], l[3],
-                 b->coords + 3 * A, b->coords + 3 * B, b->coords + 3 * C, b->coords + 3 * D,
-                 b->nprim[A], b->exps + b->prim_off[A], b->coefs + b->prim_off[A],
-                 b->nprim[B], b->exps + b->prim_off[B], b->coefs + b->prim_off[B],
-                 b->nprim[C], b->exps + b->prim_off[C], b->coefs + b->prim_off[C],
-                 b->nprim[D], b->exps + b->prim_off[D], b->coefs + b->prim_off[D],
-                 kappa, G);
+    /* position of each canonical index in the requested order; within a pair
+     * of equal l the tighter shell (larger smallest exponent) is the origin
+     * of the horizontal recurrence (see orient_first) */
+    int pos[4] = {0, 1, 2, 3};
+    if (!orient_first(b, A, B)) { pos[0] = 1; pos[1] = 0; }
+    if (!orient_first(b, C, D)) { pos[2] = 3; pos[3] = 2; }
+    if (pair_rank(l[pos[0]], l[pos[1]]) < pair_rank(l[pos[2]], l[pos[3]])) {
+        int t0 = pos[0], t1 = pos[1];
+        pos[0] = pos[2]; pos[1] = pos[3]; pos[2] = t0; pos[3] = t1;
+    }
+    int cs[4], cl[4], cn[4];
+    for (int i = 0; i < 4; ++i) { cs[i] = sh[pos[i]]; cl[i] = l[pos[i]]; cn[i] = n[pos[i]]; }
+    size_t tot = (size_t)n[0] * n[1] * n[2] * n[3];
+    double *Gc = (double *)malloc(sizeof(double) * tot);
+    double *G = (double *)malloc(sizeof(double) * tot);
+    cart_quartet(cl[0], cl[1], cl[2], cl[3],
+                 b->coords + 3 * cs[0], b->coords + 3 * cs[1], b->coords + 3 * cs[2], b->coords + 3 * cs[3],
+                 b->nprim[cs[0]], b->exps + b->prim_off[cs[0]], b->coefs + b->prim_off[cs[0]],
+                 b->nprim[cs[1]], b->exps + b->prim_off[cs[1]], b->coefs + b->prim_off[cs[1]],
+                 b->nprim[cs[2]], b->exps + b->prim_off[cs[2]], b->coefs + b->prim_off[cs[2]],
+                 b->nprim[cs[3]], b->exps + b->prim_off[cs[3]], b->coefs + b->prim_off[cs[3]],
+                 kappa, Gc);
+    /* back to the requested order (index 0 fastest) */
+    size_t cstr[4] = {1, (size_t)cn[0], (size_t)cn[0] * cn[1], (size_t)cn[0] * cn[1] * cn[2]};
+    size_t str_of_orig[4];
+    for (int i = 0; i < 4; ++i) str_of_orig[pos[i]] = cstr[i];
+    for (size_t idx = 0; idx < tot; ++idx) {
+        size_t r = idx, off = 0;
+        for (int i = 0; i < 4; ++i) { off += (r % n[i]) * str_of_orig[i]; r /= n[i]; }
+        G[idx] = Gc[off];
+    }
     transform4(G, n, T, nf, out);
-    free(G);
+    free(G); free(Gc);
     return 0;
 }
 

@@ -1,0 +1,586 @@
+!
+! Compute a batch of two-electron repulsion integrals, (AB|CD), in the Cartesian Gaussian
+! and real spherical harmonic basis.
+! Angular momenta: A=3, B=1, C=2, and D=0
+!
+! The order of the angular-dependent prefactors (x-Ra(1))**lx*(y-Ra(2))**ly*(z-Ra(3))**lz
+! is defined by the following loop:
+! I = 1
+! for lx in A..0
+!     for ly in A-lx..0
+!         lz = A-lx-ly
+!         Index[(lx,ly,lz)] = I
+!         I = I + 1
+!
+! The contracted Gaussian functions are defined as
+!
+! PhiA(lx,ly,lz) = NormA(Index[(lx,ly,lz)]) * (x-Ra(1))**lx * (y-Ra(2))**ly * (z-Ra(3))**lz * 
+!     Sum(Ga=1..NprimA) CntrA(Ga) Exp(-ExpA(Ga) * ((x-Ra(1))**2 + (y-Ra(2))**2 + (z-Ra(3))**2))
+!
+! Kappa specifies the form of the interaction potential:
+! Kappa=0 for the Coulomb interaction operator 1/r12
+! Kappa=1/Omega**2 for the screened interaction potential Erf(Omega*r12)/r12
+!
+! Code generated automatically.
+!
+module auto2e_eri_fpds
+use arithmetic
+use auto2e_KetTransfer
+use auto2e_SpherTransf
+use auto2e_WMatrix_part1
+use auto2e_WMatrix_part2
+use auto2e_WMatrix_part3
+implicit none
+
+contains
+
+subroutine auto2e_eri_3_1_2_0(G, Ra, CntrA, ExpA, NprimA, &
+Rb, CntrB, ExpB, NprimB, Rc, CntrC, ExpC, NprimC, &
+Rd, CntrD, ExpD, NprimD, Kappa)
+!
+! Two-electron integrals class: (fp|ds)
+! L-dependent normalization constants are not applied.
+! Output memory layout: CDAB
+!
+real(F64), dimension(30, *), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, ExpA, CntrB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, ExpC, CntrD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(25, 6) :: W
+!
+! Compute (LS|KS) integrals, L=3..4 and K=2..2
+!
+W = ZERO
+call auto2e_W_3_2(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 1)
+call auto2e_W_4_2(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 11, 1)
+call auto2e_BraKetTransfer_3_1_2_0(G, W, Ra, Rb)
+end subroutine auto2e_eri_3_1_2_0
+
+subroutine auto2e_eri_Spher_3_1_2_0(G, Ra, CntrA, ExpA, NprimA, &
+Rb, CntrB, ExpB, NprimB, Rc, CntrC, ExpC, NprimC, &
+Rd, CntrD, ExpD, NprimD, Kappa)
+!
+! Two-electron integrals class: (fp|ds)
+! L-dependent normalization constants are not applied.
+! Output memory layout: CDAB
+!
+real(F64), dimension(21, *), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, ExpA, CntrB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, ExpC, CntrD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(25, 6) :: W
+!
+! Compute (LS|KS) integrals, L=3..4 and K=2..2
+!
+W = ZERO
+call auto2e_W_3_2(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 1)
+call auto2e_W_4_2(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 11, 1)
+call auto2e_BraKetTransfer_Spher_3_1_2_0(G, W, Ra, Rb)
+end subroutine auto2e_eri_Spher_3_1_2_0
+
+subroutine auto2e_BraKetTransfer_3_1_2_0(G, W, Ra, Rb)
+!
+! Transform (LS|KS), L=3..4, K=2..2 using the horizontal recurrence relation
+! of Eq. 18 in Head-Gordon, M. and Pople, J.A. J. Chem. Phys. 89, 5777 (1988);
+! doi: 10.1063/1.455553
+!
+! The output integrals are expressed in the Cartesian GTOs basis.
+!
+real(F64), dimension(6, *), intent(out) :: G
+real(F64), dimension(25, 6), intent(in) :: W
+real(F64), dimension(3), intent(in) :: Ra, Rb
+real(F64), dimension(3) :: AB
+real(F64), dimension(6, 25) :: U
+AB = Ra - Rb
+U = transpose(W)
+call auto2e_KetTransfer_3_1(G(:, 1:30), U, AB(1), AB(2), AB(3))
+end subroutine auto2e_BraKetTransfer_3_1_2_0
+
+subroutine auto2e_BraKetTransfer_Spher_3_1_2_0(G, W, Ra, Rb)
+!
+! Transform (LS|KS), L=3..4, K=2..2 using the horizontal recurrence relation
+! of Eq. 18 in Head-Gordon, M. and Pople, J.A. J. Chem. Phys. 89, 5777 (1988);
+! doi: 10.1063/1.455553
+!
+! The output integrals are expressed in the real spherical harmonics basis.
+!
+real(F64), dimension(5, *), intent(out) :: G
+real(F64), dimension(25, 6), intent(in) :: W
+real(F64), dimension(3), intent(in) :: Ra, Rb
+real(F64), dimension(3) :: AB
+real(F64), dimension(25, 5) :: T
+real(F64), dimension(5, 25) :: U
+real(F64), dimension(5, 30) :: Gxyz
+AB = Ra - Rb
+call auto2e_SpherTransf_U_Vector_2_0(T, W, 25)
+U = transpose(T)
+call auto2e_KetTransfer_3_1(Gxyz, U, AB(1), AB(2), AB(3))
+call auto2e_SpherTransf_U_Vector_3_1(G(:, 1:21), Gxyz, 5)
+end subroutine auto2e_BraKetTransfer_Spher_3_1_2_0
+
+subroutine auto2e_Normalize_3_1_2_0_ABCD(Gabcd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: ABCD
+!
+real(F64), dimension(*), intent(out) :: Gabcd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 3
+do a = 1, 10
+do d = 1, 1
+do c = 1, 6
+w = a + (b-1)*10 + (c-1)*30 + (d-1)*180
+Gabcd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_3_1_2_0_ABCD
+
+subroutine auto2e_Normalize_3_1_2_0_BACD(Gbacd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: BACD
+!
+real(F64), dimension(*), intent(out) :: Gbacd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 3
+do a = 1, 10
+do d = 1, 1
+do c = 1, 6
+w = b + (a-1)*3 + (c-1)*30 + (d-1)*180
+Gbacd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_3_1_2_0_BACD
+
+subroutine auto2e_Normalize_3_1_2_0_CDAB(G, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants
+!
+real(F64), dimension(*), intent(inout) :: G
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v
+v = 1
+do b = 1, 3
+do a = 1, 10
+do d = 1, 1
+do c = 1, 6
+G(v) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*G(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_3_1_2_0_CDAB
+
+subroutine auto2e_Normalize_3_1_2_0_CDBA(Gcdba, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: CDBA
+!
+real(F64), dimension(*), intent(out) :: Gcdba
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 3
+do a = 1, 10
+do d = 1, 1
+do c = 1, 6
+w = c + (d-1)*6 + (b-1)*6 + (a-1)*18
+Gcdba(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_3_1_2_0_CDBA
+
+subroutine auto2e_Normalize_Spher_3_1_2_0_ABCD(Gabcd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: ABCD
+!
+real(F64), dimension(*), intent(out) :: Gabcd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 3
+do a = 1, 7
+do d = 1, 1
+do c = 1, 5
+w = a + (b-1)*7 + (c-1)*21 + (d-1)*105
+Gabcd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_3_1_2_0_ABCD
+
+subroutine auto2e_Normalize_Spher_3_1_2_0_BACD(Gbacd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: BACD
+!
+real(F64), dimension(*), intent(out) :: Gbacd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 3
+do a = 1, 7
+do d = 1, 1
+do c = 1, 5
+w = b + (a-1)*3 + (c-1)*21 + (d-1)*105
+Gbacd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_3_1_2_0_BACD
+
+subroutine auto2e_Normalize_Spher_3_1_2_0_CDAB(G, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants
+!
+real(F64), dimension(*), intent(inout) :: G
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v
+v = 1
+do b = 1, 3
+do a = 1, 7
+do d = 1, 1
+do c = 1, 5
+G(v) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*G(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_3_1_2_0_CDAB
+
+subroutine auto2e_Normalize_Spher_3_1_2_0_CDBA(Gcdba, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: CDBA
+!
+real(F64), dimension(*), intent(out) :: Gcdba
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 3
+do a = 1, 7
+do d = 1, 1
+do c = 1, 5
+w = c + (d-1)*5 + (b-1)*5 + (a-1)*15
+Gcdba(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_3_1_2_0_CDBA
+
+subroutine auto2e_frontend_0_2_1_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(180) :: H
+call auto2e_eri_3_1_2_0(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_3_1_2_0_ABCD(G, H, NormD, NormC, NormB, NormA)
+end subroutine auto2e_frontend_0_2_1_3
+
+subroutine auto2e_frontend_Spher_0_2_1_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(105) :: H
+call auto2e_eri_Spher_3_1_2_0(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_Spher_3_1_2_0_ABCD(G, H, NormD, NormC, NormB, NormA)
+end subroutine auto2e_frontend_Spher_0_2_1_3
+
+subroutine auto2e_frontend_3_1_0_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(180) :: H
+call auto2e_eri_3_1_2_0(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_3_1_2_0_CDBA(G, H, NormA, NormB, NormD, NormC)
+end subroutine auto2e_frontend_3_1_0_2
+
+subroutine auto2e_frontend_Spher_3_1_0_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(105) :: H
+call auto2e_eri_Spher_3_1_2_0(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_Spher_3_1_2_0_CDBA(G, H, NormA, NormB, NormD, NormC)
+end subroutine auto2e_frontend_Spher_3_1_0_2
+
+subroutine auto2e_frontend_2_0_3_1(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(180) :: H
+call auto2e_eri_3_1_2_0(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_3_1_2_0_BACD(G, H, NormC, NormD, NormA, NormB)
+end subroutine auto2e_frontend_2_0_3_1
+
+subroutine auto2e_frontend_Spher_2_0_3_1(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(105) :: H
+call auto2e_eri_Spher_3_1_2_0(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_Spher_3_1_2_0_BACD(G, H, NormC, NormD, NormA, NormB)
+end subroutine auto2e_frontend_Spher_2_0_3_1
+
+subroutine auto2e_frontend_1_3_0_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+call auto2e_eri_3_1_2_0(G, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_3_1_2_0_CDAB(G, NormB, NormA, NormD, NormC)
+end subroutine auto2e_frontend_1_3_0_2
+
+subroutine auto2e_frontend_Spher_1_3_0_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+call auto2e_eri_Spher_3_1_2_0(G, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_Spher_3_1_2_0_CDAB(G, NormB, NormA, NormD, NormC)
+end subroutine auto2e_frontend_Spher_1_3_0_2
+
+subroutine auto2e_frontend_0_2_3_1(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(180) :: H
+call auto2e_eri_3_1_2_0(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_3_1_2_0_BACD(G, H, NormC, NormD, NormB, NormA)
+end subroutine auto2e_frontend_0_2_3_1
+
+subroutine auto2e_frontend_Spher_0_2_3_1(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(105) :: H
+call auto2e_eri_Spher_3_1_2_0(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_Spher_3_1_2_0_BACD(G, H, NormC, NormD, NormB, NormA)
+end subroutine auto2e_frontend_Spher_0_2_3_1
+
+subroutine auto2e_frontend_2_0_1_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(180) :: H
+call auto2e_eri_3_1_2_0(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_3_1_2_0_ABCD(G, H, NormD, NormC, NormA, NormB)
+end subroutine auto2e_frontend_2_0_1_3
+
+subroutine auto2e_frontend_Spher_2_0_1_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(105) :: H
+call auto2e_eri_Spher_3_1_2_0(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_Spher_3_1_2_0_ABCD(G, H, NormD, NormC, NormA, NormB)
+end subroutine auto2e_frontend_Spher_2_0_1_3
+
+subroutine auto2e_frontend_1_3_2_0(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+call auto2e_eri_3_1_2_0(G, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_3_1_2_0_CDAB(G, NormB, NormA, NormC, NormD)
+end subroutine auto2e_frontend_1_3_2_0
+
+subroutine auto2e_frontend_Spher_1_3_2_0(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+call auto2e_eri_Spher_3_1_2_0(G, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_Spher_3_1_2_0_CDAB(G, NormB, NormA, NormC, NormD)
+end subroutine auto2e_frontend_Spher_1_3_2_0
+
+subroutine auto2e_frontend_3_1_2_0(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(180) :: H
+call auto2e_eri_3_1_2_0(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_3_1_2_0_CDBA(G, H, NormA, NormB, NormC, NormD)
+end subroutine auto2e_frontend_3_1_2_0
+
+subroutine auto2e_frontend_Spher_3_1_2_0(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(105) :: H
+call auto2e_eri_Spher_3_1_2_0(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_Spher_3_1_2_0_CDBA(G, H, NormA, NormB, NormC, NormD)
+end subroutine auto2e_frontend_Spher_3_1_2_0
+end module auto2e_eri_fpds

@@ -1,0 +1,834 @@
+!
+! Compute a batch of two-electron repulsion integrals, (AB|CD), in the Cartesian Gaussian
+! and real spherical harmonic basis.
+! Angular momenta: A=4, B=3, C=4, and D=2
+!
+! The order of the angular-dependent prefactors (x-Ra(1))**lx*(y-Ra(2))**ly*(z-Ra(3))**lz
+! is defined by the following loop:
+! I = 1
+! for lx in A..0
+!     for ly in A-lx..0
+!         lz = A-lx-ly
+!         Index[(lx,ly,lz)] = I
+!         I = I + 1
+!
+! The contracted Gaussian functions are defined as
+!
+! PhiA(lx,ly,lz) = NormA(Index[(lx,ly,lz)]) * (x-Ra(1))**lx * (y-Ra(2))**ly * (z-Ra(3))**lz * 
+!     Sum(Ga=1..NprimA) CntrA(Ga) Exp(-ExpA(Ga) * ((x-Ra(1))**2 + (y-Ra(2))**2 + (z-Ra(3))**2))
+!
+! Kappa specifies the form of the interaction potential:
+! Kappa=0 for the Coulomb interaction operator 1/r12
+! Kappa=1/Omega**2 for the screened interaction potential Erf(Omega*r12)/r12
+!
+! Code generated automatically.
+!
+module auto2e_eri_gfgd
+use arithmetic
+use auto2e_KetTransfer
+use auto2e_SpherTransf
+use auto2e_WMatrix_part1
+use auto2e_WMatrix_part2
+use auto2e_WMatrix_part3
+implicit none
+
+contains
+
+subroutine auto2e_eri_4_3_4_2(G, Ra, CntrA, ExpA, NprimA, &
+Rb, CntrB, ExpB, NprimB, Rc, CntrC, ExpC, NprimC, &
+Rd, CntrD, ExpD, NprimD, Kappa)
+!
+! Two-electron integrals class: (gf|gd)
+! L-dependent normalization constants are not applied.
+! Output memory layout: CDAB
+!
+real(F64), dimension(150, *), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, ExpA, CntrB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, ExpC, CntrD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(100, 64) :: W
+!
+! Compute (LS|KS) integrals, L=4..7 and K=4..6
+!
+W = ZERO
+call auto2e_W_4_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 1)
+call auto2e_W_5_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 16, 1)
+call auto2e_W_6_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 37, 1)
+call auto2e_W_7_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 65, 1)
+call auto2e_W_4_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 16)
+call auto2e_W_5_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 16, 16)
+call auto2e_W_6_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 37, 16)
+call auto2e_W_7_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 65, 16)
+call auto2e_W_4_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 37)
+call auto2e_W_5_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 16, 37)
+call auto2e_W_6_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 37, 37)
+call auto2e_W_7_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 65, 37)
+call auto2e_BraKetTransfer_4_3_4_2(G, W, Ra, Rb, Rc, Rd)
+end subroutine auto2e_eri_4_3_4_2
+
+subroutine auto2e_eri_Spher_4_3_4_2(G, Ra, CntrA, ExpA, NprimA, &
+Rb, CntrB, ExpB, NprimB, Rc, CntrC, ExpC, NprimC, &
+Rd, CntrD, ExpD, NprimD, Kappa)
+!
+! Two-electron integrals class: (gf|gd)
+! L-dependent normalization constants are not applied.
+! Output memory layout: CDAB
+!
+real(F64), dimension(63, *), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, ExpA, CntrB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, ExpC, CntrD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(100, 64) :: W
+!
+! Compute (LS|KS) integrals, L=4..7 and K=4..6
+!
+W = ZERO
+call auto2e_W_4_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 1)
+call auto2e_W_5_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 16, 1)
+call auto2e_W_6_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 37, 1)
+call auto2e_W_7_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 65, 1)
+call auto2e_W_4_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 16)
+call auto2e_W_5_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 16, 16)
+call auto2e_W_6_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 37, 16)
+call auto2e_W_7_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 65, 16)
+call auto2e_W_4_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 37)
+call auto2e_W_5_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 16, 37)
+call auto2e_W_6_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 37, 37)
+call auto2e_W_7_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 65, 37)
+call auto2e_BraKetTransfer_Spher_4_3_4_2(G, W, Ra, Rb, Rc, Rd)
+end subroutine auto2e_eri_Spher_4_3_4_2
+
+subroutine auto2e_BraKetTransfer_4_3_4_2(G, W, Ra, Rb, Rc, Rd)
+!
+! Transform (LS|KS), L=4..7, K=4..6 using the horizontal recurrence relation
+! of Eq. 18 in Head-Gordon, M. and Pople, J.A. J. Chem. Phys. 89, 5777 (1988);
+! doi: 10.1063/1.455553
+!
+! The output integrals are expressed in the Cartesian GTOs basis.
+!
+real(F64), dimension(90, *), intent(out) :: G
+real(F64), dimension(100, 64), intent(in) :: W
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(3) :: AB, CD
+real(F64), dimension(100, 90) :: T
+real(F64), dimension(90, 100) :: U
+AB = Ra - Rb
+CD = Rc - Rd
+call auto2e_KetTransfer_4_2(T, W, CD(1), CD(2), CD(3))
+U = transpose(T)
+call auto2e_KetTransfer_4_3(G(:, 1:150), U, AB(1), AB(2), AB(3))
+end subroutine auto2e_BraKetTransfer_4_3_4_2
+
+subroutine auto2e_BraKetTransfer_Spher_4_3_4_2(G, W, Ra, Rb, Rc, Rd)
+!
+! Transform (LS|KS), L=4..7, K=4..6 using the horizontal recurrence relation
+! of Eq. 18 in Head-Gordon, M. and Pople, J.A. J. Chem. Phys. 89, 5777 (1988);
+! doi: 10.1063/1.455553
+!
+! The output integrals are expressed in the real spherical harmonics basis.
+!
+real(F64), dimension(45, *), intent(out) :: G
+real(F64), dimension(100, 64), intent(in) :: W
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(3) :: AB, CD
+real(F64), dimension(100, 90) :: Txyz
+real(F64), dimension(100, 45) :: T
+real(F64), dimension(45, 100) :: U
+real(F64), dimension(45, 150) :: Gxyz
+AB = Ra - Rb
+CD = Rc - Rd
+call auto2e_KetTransfer_4_2(Txyz, W, CD(1), CD(2), CD(3))
+call auto2e_SpherTransf_U_Vector_4_2(T, Txyz, 100)
+U = transpose(T)
+call auto2e_KetTransfer_4_3(Gxyz, U, AB(1), AB(2), AB(3))
+call auto2e_SpherTransf_U_Vector_4_3(G(:, 1:63), Gxyz, 45)
+end subroutine auto2e_BraKetTransfer_Spher_4_3_4_2
+
+subroutine auto2e_Normalize_4_3_4_2_ABCD(Gabcd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: ABCD
+!
+real(F64), dimension(*), intent(out) :: Gabcd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 10
+do a = 1, 15
+do d = 1, 6
+do c = 1, 15
+w = a + (b-1)*15 + (c-1)*150 + (d-1)*2250
+Gabcd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_4_3_4_2_ABCD
+
+subroutine auto2e_Normalize_4_3_4_2_ABDC(Gabdc, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: ABDC
+!
+real(F64), dimension(*), intent(out) :: Gabdc
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 10
+do a = 1, 15
+do d = 1, 6
+do c = 1, 15
+w = a + (b-1)*15 + (d-1)*150 + (c-1)*900
+Gabdc(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_4_3_4_2_ABDC
+
+subroutine auto2e_Normalize_4_3_4_2_BACD(Gbacd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: BACD
+!
+real(F64), dimension(*), intent(out) :: Gbacd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 10
+do a = 1, 15
+do d = 1, 6
+do c = 1, 15
+w = b + (a-1)*10 + (c-1)*150 + (d-1)*2250
+Gbacd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_4_3_4_2_BACD
+
+subroutine auto2e_Normalize_4_3_4_2_BADC(Gbadc, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: BADC
+!
+real(F64), dimension(*), intent(out) :: Gbadc
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 10
+do a = 1, 15
+do d = 1, 6
+do c = 1, 15
+w = b + (a-1)*10 + (d-1)*150 + (c-1)*900
+Gbadc(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_4_3_4_2_BADC
+
+subroutine auto2e_Normalize_4_3_4_2_CDAB(G, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants
+!
+real(F64), dimension(*), intent(inout) :: G
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v
+v = 1
+do b = 1, 10
+do a = 1, 15
+do d = 1, 6
+do c = 1, 15
+G(v) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*G(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_4_3_4_2_CDAB
+
+subroutine auto2e_Normalize_4_3_4_2_CDBA(Gcdba, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: CDBA
+!
+real(F64), dimension(*), intent(out) :: Gcdba
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 10
+do a = 1, 15
+do d = 1, 6
+do c = 1, 15
+w = c + (d-1)*15 + (b-1)*90 + (a-1)*900
+Gcdba(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_4_3_4_2_CDBA
+
+subroutine auto2e_Normalize_4_3_4_2_DCAB(Gdcab, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: DCAB
+!
+real(F64), dimension(*), intent(out) :: Gdcab
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 10
+do a = 1, 15
+do d = 1, 6
+do c = 1, 15
+w = d + (c-1)*6 + (a-1)*90 + (b-1)*1350
+Gdcab(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_4_3_4_2_DCAB
+
+subroutine auto2e_Normalize_4_3_4_2_DCBA(Gdcba, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: DCBA
+!
+real(F64), dimension(*), intent(out) :: Gdcba
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 10
+do a = 1, 15
+do d = 1, 6
+do c = 1, 15
+w = d + (c-1)*6 + (b-1)*90 + (a-1)*900
+Gdcba(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_4_3_4_2_DCBA
+
+subroutine auto2e_Normalize_Spher_4_3_4_2_ABCD(Gabcd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: ABCD
+!
+real(F64), dimension(*), intent(out) :: Gabcd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 7
+do a = 1, 9
+do d = 1, 5
+do c = 1, 9
+w = a + (b-1)*9 + (c-1)*63 + (d-1)*567
+Gabcd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_4_3_4_2_ABCD
+
+subroutine auto2e_Normalize_Spher_4_3_4_2_ABDC(Gabdc, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: ABDC
+!
+real(F64), dimension(*), intent(out) :: Gabdc
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 7
+do a = 1, 9
+do d = 1, 5
+do c = 1, 9
+w = a + (b-1)*9 + (d-1)*63 + (c-1)*315
+Gabdc(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_4_3_4_2_ABDC
+
+subroutine auto2e_Normalize_Spher_4_3_4_2_BACD(Gbacd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: BACD
+!
+real(F64), dimension(*), intent(out) :: Gbacd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 7
+do a = 1, 9
+do d = 1, 5
+do c = 1, 9
+w = b + (a-1)*7 + (c-1)*63 + (d-1)*567
+Gbacd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_4_3_4_2_BACD
+
+subroutine auto2e_Normalize_Spher_4_3_4_2_BADC(Gbadc, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: BADC
+!
+real(F64), dimension(*), intent(out) :: Gbadc
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 7
+do a = 1, 9
+do d = 1, 5
+do c = 1, 9
+w = b + (a-1)*7 + (d-1)*63 + (c-1)*315
+Gbadc(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_4_3_4_2_BADC
+
+subroutine auto2e_Normalize_Spher_4_3_4_2_CDAB(G, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants
+!
+real(F64), dimension(*), intent(inout) :: G
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v
+v = 1
+do b = 1, 7
+do a = 1, 9
+do d = 1, 5
+do c = 1, 9
+G(v) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*G(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_4_3_4_2_CDAB
+
+subroutine auto2e_Normalize_Spher_4_3_4_2_CDBA(Gcdba, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: CDBA
+!
+real(F64), dimension(*), intent(out) :: Gcdba
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 7
+do a = 1, 9
+do d = 1, 5
+do c = 1, 9
+w = c + (d-1)*9 + (b-1)*45 + (a-1)*315
+Gcdba(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_4_3_4_2_CDBA
+
+subroutine auto2e_Normalize_Spher_4_3_4_2_DCAB(Gdcab, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: DCAB
+!
+real(F64), dimension(*), intent(out) :: Gdcab
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 7
+do a = 1, 9
+do d = 1, 5
+do c = 1, 9
+w = d + (c-1)*5 + (a-1)*45 + (b-1)*405
+Gdcab(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_4_3_4_2_DCAB
+
+subroutine auto2e_Normalize_Spher_4_3_4_2_DCBA(Gdcba, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: DCBA
+!
+real(F64), dimension(*), intent(out) :: Gdcba
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 7
+do a = 1, 9
+do d = 1, 5
+do c = 1, 9
+w = d + (c-1)*5 + (b-1)*45 + (a-1)*315
+Gdcba(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_4_3_4_2_DCBA
+
+subroutine auto2e_frontend_2_4_4_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(13500) :: H
+call auto2e_eri_4_3_4_2(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_4_3_4_2_BACD(G, H, NormC, NormD, NormB, NormA)
+end subroutine auto2e_frontend_2_4_4_3
+
+subroutine auto2e_frontend_Spher_2_4_4_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(2835) :: H
+call auto2e_eri_Spher_4_3_4_2(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_Spher_4_3_4_2_BACD(G, H, NormC, NormD, NormB, NormA)
+end subroutine auto2e_frontend_Spher_2_4_4_3
+
+subroutine auto2e_frontend_3_4_4_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(13500) :: H
+call auto2e_eri_4_3_4_2(H, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_4_3_4_2_DCAB(G, H, NormB, NormA, NormC, NormD)
+end subroutine auto2e_frontend_3_4_4_2
+
+subroutine auto2e_frontend_Spher_3_4_4_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(2835) :: H
+call auto2e_eri_Spher_4_3_4_2(H, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_Spher_4_3_4_2_DCAB(G, H, NormB, NormA, NormC, NormD)
+end subroutine auto2e_frontend_Spher_3_4_4_2
+
+subroutine auto2e_frontend_3_4_2_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+call auto2e_eri_4_3_4_2(G, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_4_3_4_2_CDAB(G, NormB, NormA, NormD, NormC)
+end subroutine auto2e_frontend_3_4_2_4
+
+subroutine auto2e_frontend_Spher_3_4_2_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+call auto2e_eri_Spher_4_3_4_2(G, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_Spher_4_3_4_2_CDAB(G, NormB, NormA, NormD, NormC)
+end subroutine auto2e_frontend_Spher_3_4_2_4
+
+subroutine auto2e_frontend_4_2_3_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(13500) :: H
+call auto2e_eri_4_3_4_2(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_4_3_4_2_ABDC(G, H, NormD, NormC, NormA, NormB)
+end subroutine auto2e_frontend_4_2_3_4
+
+subroutine auto2e_frontend_Spher_4_2_3_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(2835) :: H
+call auto2e_eri_Spher_4_3_4_2(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_Spher_4_3_4_2_ABDC(G, H, NormD, NormC, NormA, NormB)
+end subroutine auto2e_frontend_Spher_4_2_3_4
+
+subroutine auto2e_frontend_4_3_4_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(13500) :: H
+call auto2e_eri_4_3_4_2(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_4_3_4_2_DCBA(G, H, NormA, NormB, NormC, NormD)
+end subroutine auto2e_frontend_4_3_4_2
+
+subroutine auto2e_frontend_Spher_4_3_4_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(2835) :: H
+call auto2e_eri_Spher_4_3_4_2(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_Spher_4_3_4_2_DCBA(G, H, NormA, NormB, NormC, NormD)
+end subroutine auto2e_frontend_Spher_4_3_4_2
+
+subroutine auto2e_frontend_2_4_3_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(13500) :: H
+call auto2e_eri_4_3_4_2(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_4_3_4_2_ABCD(G, H, NormD, NormC, NormB, NormA)
+end subroutine auto2e_frontend_2_4_3_4
+
+subroutine auto2e_frontend_Spher_2_4_3_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(2835) :: H
+call auto2e_eri_Spher_4_3_4_2(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_Spher_4_3_4_2_ABCD(G, H, NormD, NormC, NormB, NormA)
+end subroutine auto2e_frontend_Spher_2_4_3_4
+
+subroutine auto2e_frontend_4_3_2_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(13500) :: H
+call auto2e_eri_4_3_4_2(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_4_3_4_2_CDBA(G, H, NormA, NormB, NormD, NormC)
+end subroutine auto2e_frontend_4_3_2_4
+
+subroutine auto2e_frontend_Spher_4_3_2_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(2835) :: H
+call auto2e_eri_Spher_4_3_4_2(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_Spher_4_3_4_2_CDBA(G, H, NormA, NormB, NormD, NormC)
+end subroutine auto2e_frontend_Spher_4_3_2_4
+
+subroutine auto2e_frontend_4_2_4_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(13500) :: H
+call auto2e_eri_4_3_4_2(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_4_3_4_2_BADC(G, H, NormC, NormD, NormA, NormB)
+end subroutine auto2e_frontend_4_2_4_3
+
+subroutine auto2e_frontend_Spher_4_2_4_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(2835) :: H
+call auto2e_eri_Spher_4_3_4_2(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_Spher_4_3_4_2_BADC(G, H, NormC, NormD, NormA, NormB)
+end subroutine auto2e_frontend_Spher_4_2_4_3
+end module auto2e_eri_gfgd

@@ -1,0 +1,834 @@
+!
+! Compute a batch of two-electron repulsion integrals, (AB|CD), in the Cartesian Gaussian
+! and real spherical harmonic basis.
+! Angular momenta: A=5, B=2, C=4, and D=3
+!
+! The order of the angular-dependent prefactors (x-Ra(1))**lx*(y-Ra(2))**ly*(z-Ra(3))**lz
+! is defined by the following loop:
+! I = 1
+! for lx in A..0
+!     for ly in A-lx..0
+!         lz = A-lx-ly
+!         Index[(lx,ly,lz)] = I
+!         I = I + 1
+!
+! The contracted Gaussian functions are defined as
+!
+! PhiA(lx,ly,lz) = NormA(Index[(lx,ly,lz)]) * (x-Ra(1))**lx * (y-Ra(2))**ly * (z-Ra(3))**lz * 
+!     Sum(Ga=1..NprimA) CntrA(Ga) Exp(-ExpA(Ga) * ((x-Ra(1))**2 + (y-Ra(2))**2 + (z-Ra(3))**2))
+!
+! Kappa specifies the form of the interaction potential:
+! Kappa=0 for the Coulomb interaction operator 1/r12
+! Kappa=1/Omega**2 for the screened interaction potential Erf(Omega*r12)/r12
+!
+! Code generated automatically.
+!
+module auto2e_eri_hdgf
+use arithmetic
+use auto2e_KetTransfer
+use auto2e_SpherTransf
+use auto2e_WMatrix_part1
+use auto2e_WMatrix_part2
+use auto2e_WMatrix_part3
+implicit none
+
+contains
+
+subroutine auto2e_eri_5_2_4_3(G, Ra, CntrA, ExpA, NprimA, &
+Rb, CntrB, ExpB, NprimB, Rc, CntrC, ExpC, NprimC, &
+Rd, CntrD, ExpD, NprimD, Kappa)
+!
+! Two-electron integrals class: (hd|gf)
+! L-dependent normalization constants are not applied.
+! Output memory layout: CDAB
+!
+real(F64), dimension(126, *), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, ExpA, CntrB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, ExpC, CntrD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(85, 100) :: W
+!
+! Compute (LS|KS) integrals, L=5..7 and K=4..7
+!
+W = ZERO
+call auto2e_W_5_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 1)
+call auto2e_W_6_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 22, 1)
+call auto2e_W_7_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 50, 1)
+call auto2e_W_5_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 16)
+call auto2e_W_6_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 22, 16)
+call auto2e_W_7_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 50, 16)
+call auto2e_W_5_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 37)
+call auto2e_W_6_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 22, 37)
+call auto2e_W_7_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 50, 37)
+call auto2e_W_5_7(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 65)
+call auto2e_W_6_7(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 22, 65)
+call auto2e_W_7_7(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 50, 65)
+call auto2e_BraKetTransfer_5_2_4_3(G, W, Ra, Rb, Rc, Rd)
+end subroutine auto2e_eri_5_2_4_3
+
+subroutine auto2e_eri_Spher_5_2_4_3(G, Ra, CntrA, ExpA, NprimA, &
+Rb, CntrB, ExpB, NprimB, Rc, CntrC, ExpC, NprimC, &
+Rd, CntrD, ExpD, NprimD, Kappa)
+!
+! Two-electron integrals class: (hd|gf)
+! L-dependent normalization constants are not applied.
+! Output memory layout: CDAB
+!
+real(F64), dimension(55, *), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, ExpA, CntrB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, ExpC, CntrD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(85, 100) :: W
+!
+! Compute (LS|KS) integrals, L=5..7 and K=4..7
+!
+W = ZERO
+call auto2e_W_5_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 1)
+call auto2e_W_6_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 22, 1)
+call auto2e_W_7_4(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 50, 1)
+call auto2e_W_5_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 16)
+call auto2e_W_6_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 22, 16)
+call auto2e_W_7_5(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 50, 16)
+call auto2e_W_5_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 37)
+call auto2e_W_6_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 22, 37)
+call auto2e_W_7_6(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 50, 37)
+call auto2e_W_5_7(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 65)
+call auto2e_W_6_7(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 22, 65)
+call auto2e_W_7_7(W, Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 50, 65)
+call auto2e_BraKetTransfer_Spher_5_2_4_3(G, W, Ra, Rb, Rc, Rd)
+end subroutine auto2e_eri_Spher_5_2_4_3
+
+subroutine auto2e_BraKetTransfer_5_2_4_3(G, W, Ra, Rb, Rc, Rd)
+!
+! Transform (LS|KS), L=5..7, K=4..7 using the horizontal recurrence relation
+! of Eq. 18 in Head-Gordon, M. and Pople, J.A. J. Chem. Phys. 89, 5777 (1988);
+! doi: 10.1063/1.455553
+!
+! The output integrals are expressed in the Cartesian GTOs basis.
+!
+real(F64), dimension(150, *), intent(out) :: G
+real(F64), dimension(85, 100), intent(in) :: W
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(3) :: AB, CD
+real(F64), dimension(85, 150) :: T
+real(F64), dimension(150, 85) :: U
+AB = Ra - Rb
+CD = Rc - Rd
+call auto2e_KetTransfer_4_3(T, W, CD(1), CD(2), CD(3))
+U = transpose(T)
+call auto2e_KetTransfer_5_2(G(:, 1:126), U, AB(1), AB(2), AB(3))
+end subroutine auto2e_BraKetTransfer_5_2_4_3
+
+subroutine auto2e_BraKetTransfer_Spher_5_2_4_3(G, W, Ra, Rb, Rc, Rd)
+!
+! Transform (LS|KS), L=5..7, K=4..7 using the horizontal recurrence relation
+! of Eq. 18 in Head-Gordon, M. and Pople, J.A. J. Chem. Phys. 89, 5777 (1988);
+! doi: 10.1063/1.455553
+!
+! The output integrals are expressed in the real spherical harmonics basis.
+!
+real(F64), dimension(63, *), intent(out) :: G
+real(F64), dimension(85, 100), intent(in) :: W
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(3) :: AB, CD
+real(F64), dimension(85, 150) :: Txyz
+real(F64), dimension(85, 63) :: T
+real(F64), dimension(63, 85) :: U
+real(F64), dimension(63, 126) :: Gxyz
+AB = Ra - Rb
+CD = Rc - Rd
+call auto2e_KetTransfer_4_3(Txyz, W, CD(1), CD(2), CD(3))
+call auto2e_SpherTransf_U_Vector_4_3(T, Txyz, 85)
+U = transpose(T)
+call auto2e_KetTransfer_5_2(Gxyz, U, AB(1), AB(2), AB(3))
+call auto2e_SpherTransf_U_Vector_5_2(G(:, 1:55), Gxyz, 63)
+end subroutine auto2e_BraKetTransfer_Spher_5_2_4_3
+
+subroutine auto2e_Normalize_5_2_4_3_ABCD(Gabcd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: ABCD
+!
+real(F64), dimension(*), intent(out) :: Gabcd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 6
+do a = 1, 21
+do d = 1, 10
+do c = 1, 15
+w = a + (b-1)*21 + (c-1)*126 + (d-1)*1890
+Gabcd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_5_2_4_3_ABCD
+
+subroutine auto2e_Normalize_5_2_4_3_ABDC(Gabdc, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: ABDC
+!
+real(F64), dimension(*), intent(out) :: Gabdc
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 6
+do a = 1, 21
+do d = 1, 10
+do c = 1, 15
+w = a + (b-1)*21 + (d-1)*126 + (c-1)*1260
+Gabdc(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_5_2_4_3_ABDC
+
+subroutine auto2e_Normalize_5_2_4_3_BACD(Gbacd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: BACD
+!
+real(F64), dimension(*), intent(out) :: Gbacd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 6
+do a = 1, 21
+do d = 1, 10
+do c = 1, 15
+w = b + (a-1)*6 + (c-1)*126 + (d-1)*1890
+Gbacd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_5_2_4_3_BACD
+
+subroutine auto2e_Normalize_5_2_4_3_BADC(Gbadc, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: BADC
+!
+real(F64), dimension(*), intent(out) :: Gbadc
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 6
+do a = 1, 21
+do d = 1, 10
+do c = 1, 15
+w = b + (a-1)*6 + (d-1)*126 + (c-1)*1260
+Gbadc(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_5_2_4_3_BADC
+
+subroutine auto2e_Normalize_5_2_4_3_CDAB(G, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants
+!
+real(F64), dimension(*), intent(inout) :: G
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v
+v = 1
+do b = 1, 6
+do a = 1, 21
+do d = 1, 10
+do c = 1, 15
+G(v) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*G(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_5_2_4_3_CDAB
+
+subroutine auto2e_Normalize_5_2_4_3_CDBA(Gcdba, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: CDBA
+!
+real(F64), dimension(*), intent(out) :: Gcdba
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 6
+do a = 1, 21
+do d = 1, 10
+do c = 1, 15
+w = c + (d-1)*15 + (b-1)*150 + (a-1)*900
+Gcdba(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_5_2_4_3_CDBA
+
+subroutine auto2e_Normalize_5_2_4_3_DCAB(Gdcab, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: DCAB
+!
+real(F64), dimension(*), intent(out) :: Gdcab
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 6
+do a = 1, 21
+do d = 1, 10
+do c = 1, 15
+w = d + (c-1)*10 + (a-1)*150 + (b-1)*3150
+Gdcab(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_5_2_4_3_DCAB
+
+subroutine auto2e_Normalize_5_2_4_3_DCBA(Gdcba, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: DCBA
+!
+real(F64), dimension(*), intent(out) :: Gdcba
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 6
+do a = 1, 21
+do d = 1, 10
+do c = 1, 15
+w = d + (c-1)*10 + (b-1)*150 + (a-1)*900
+Gdcba(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_5_2_4_3_DCBA
+
+subroutine auto2e_Normalize_Spher_5_2_4_3_ABCD(Gabcd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: ABCD
+!
+real(F64), dimension(*), intent(out) :: Gabcd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 5
+do a = 1, 11
+do d = 1, 7
+do c = 1, 9
+w = a + (b-1)*11 + (c-1)*55 + (d-1)*495
+Gabcd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_5_2_4_3_ABCD
+
+subroutine auto2e_Normalize_Spher_5_2_4_3_ABDC(Gabdc, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: ABDC
+!
+real(F64), dimension(*), intent(out) :: Gabdc
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 5
+do a = 1, 11
+do d = 1, 7
+do c = 1, 9
+w = a + (b-1)*11 + (d-1)*55 + (c-1)*385
+Gabdc(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_5_2_4_3_ABDC
+
+subroutine auto2e_Normalize_Spher_5_2_4_3_BACD(Gbacd, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: BACD
+!
+real(F64), dimension(*), intent(out) :: Gbacd
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 5
+do a = 1, 11
+do d = 1, 7
+do c = 1, 9
+w = b + (a-1)*5 + (c-1)*55 + (d-1)*495
+Gbacd(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_5_2_4_3_BACD
+
+subroutine auto2e_Normalize_Spher_5_2_4_3_BADC(Gbadc, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: BADC
+!
+real(F64), dimension(*), intent(out) :: Gbadc
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 5
+do a = 1, 11
+do d = 1, 7
+do c = 1, 9
+w = b + (a-1)*5 + (d-1)*55 + (c-1)*385
+Gbadc(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_5_2_4_3_BADC
+
+subroutine auto2e_Normalize_Spher_5_2_4_3_CDAB(G, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants
+!
+real(F64), dimension(*), intent(inout) :: G
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v
+v = 1
+do b = 1, 5
+do a = 1, 11
+do d = 1, 7
+do c = 1, 9
+G(v) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*G(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_5_2_4_3_CDAB
+
+subroutine auto2e_Normalize_Spher_5_2_4_3_CDBA(Gcdba, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: CDBA
+!
+real(F64), dimension(*), intent(out) :: Gcdba
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 5
+do a = 1, 11
+do d = 1, 7
+do c = 1, 9
+w = c + (d-1)*9 + (b-1)*63 + (a-1)*315
+Gcdba(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_5_2_4_3_CDBA
+
+subroutine auto2e_Normalize_Spher_5_2_4_3_DCAB(Gdcab, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: DCAB
+!
+real(F64), dimension(*), intent(out) :: Gdcab
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 5
+do a = 1, 11
+do d = 1, 7
+do c = 1, 9
+w = d + (c-1)*7 + (a-1)*63 + (b-1)*693
+Gdcab(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_5_2_4_3_DCAB
+
+subroutine auto2e_Normalize_Spher_5_2_4_3_DCBA(Gdcba, Gcdab, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: CDAB
+! Output memory layout: DCBA
+!
+real(F64), dimension(*), intent(out) :: Gdcba
+real(F64), dimension(*), intent(in) :: Gcdab
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do b = 1, 5
+do a = 1, 11
+do d = 1, 7
+do c = 1, 9
+w = d + (c-1)*7 + (b-1)*63 + (a-1)*315
+Gdcba(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gcdab(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_Spher_5_2_4_3_DCBA
+
+subroutine auto2e_frontend_2_5_3_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+call auto2e_eri_5_2_4_3(G, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_5_2_4_3_CDAB(G, NormB, NormA, NormD, NormC)
+end subroutine auto2e_frontend_2_5_3_4
+
+subroutine auto2e_frontend_Spher_2_5_3_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+call auto2e_eri_Spher_5_2_4_3(G, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_Spher_5_2_4_3_CDAB(G, NormB, NormA, NormD, NormC)
+end subroutine auto2e_frontend_Spher_2_5_3_4
+
+subroutine auto2e_frontend_3_4_2_5(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(18900) :: H
+call auto2e_eri_5_2_4_3(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_5_2_4_3_ABCD(G, H, NormD, NormC, NormB, NormA)
+end subroutine auto2e_frontend_3_4_2_5
+
+subroutine auto2e_frontend_Spher_3_4_2_5(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(3465) :: H
+call auto2e_eri_Spher_5_2_4_3(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_Spher_5_2_4_3_ABCD(G, H, NormD, NormC, NormB, NormA)
+end subroutine auto2e_frontend_Spher_3_4_2_5
+
+subroutine auto2e_frontend_5_2_4_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(18900) :: H
+call auto2e_eri_5_2_4_3(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_5_2_4_3_DCBA(G, H, NormA, NormB, NormC, NormD)
+end subroutine auto2e_frontend_5_2_4_3
+
+subroutine auto2e_frontend_Spher_5_2_4_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(3465) :: H
+call auto2e_eri_Spher_5_2_4_3(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_Spher_5_2_4_3_DCBA(G, H, NormA, NormB, NormC, NormD)
+end subroutine auto2e_frontend_Spher_5_2_4_3
+
+subroutine auto2e_frontend_3_4_5_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(18900) :: H
+call auto2e_eri_5_2_4_3(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_5_2_4_3_BACD(G, H, NormC, NormD, NormB, NormA)
+end subroutine auto2e_frontend_3_4_5_2
+
+subroutine auto2e_frontend_Spher_3_4_5_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(3465) :: H
+call auto2e_eri_Spher_5_2_4_3(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, Kappa)
+call auto2e_Normalize_Spher_5_2_4_3_BACD(G, H, NormC, NormD, NormB, NormA)
+end subroutine auto2e_frontend_Spher_3_4_5_2
+
+subroutine auto2e_frontend_5_2_3_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(18900) :: H
+call auto2e_eri_5_2_4_3(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_5_2_4_3_CDBA(G, H, NormA, NormB, NormD, NormC)
+end subroutine auto2e_frontend_5_2_3_4
+
+subroutine auto2e_frontend_Spher_5_2_3_4(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(3465) :: H
+call auto2e_eri_Spher_5_2_4_3(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_Spher_5_2_4_3_CDBA(G, H, NormA, NormB, NormD, NormC)
+end subroutine auto2e_frontend_Spher_5_2_3_4
+
+subroutine auto2e_frontend_2_5_4_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(18900) :: H
+call auto2e_eri_5_2_4_3(H, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_5_2_4_3_DCAB(G, H, NormB, NormA, NormC, NormD)
+end subroutine auto2e_frontend_2_5_4_3
+
+subroutine auto2e_frontend_Spher_2_5_4_3(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(3465) :: H
+call auto2e_eri_Spher_5_2_4_3(H, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_Spher_5_2_4_3_DCAB(G, H, NormB, NormA, NormC, NormD)
+end subroutine auto2e_frontend_Spher_2_5_4_3
+
+subroutine auto2e_frontend_4_3_2_5(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(18900) :: H
+call auto2e_eri_5_2_4_3(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_5_2_4_3_ABDC(G, H, NormD, NormC, NormA, NormB)
+end subroutine auto2e_frontend_4_3_2_5
+
+subroutine auto2e_frontend_Spher_4_3_2_5(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(3465) :: H
+call auto2e_eri_Spher_5_2_4_3(H, Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_Spher_5_2_4_3_ABDC(G, H, NormD, NormC, NormA, NormB)
+end subroutine auto2e_frontend_Spher_4_3_2_5
+
+subroutine auto2e_frontend_4_3_5_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(18900) :: H
+call auto2e_eri_5_2_4_3(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_5_2_4_3_BADC(G, H, NormC, NormD, NormA, NormB)
+end subroutine auto2e_frontend_4_3_5_2
+
+subroutine auto2e_frontend_Spher_4_3_5_2(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(3465) :: H
+call auto2e_eri_Spher_5_2_4_3(H, Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, Kappa)
+call auto2e_Normalize_Spher_5_2_4_3_BADC(G, H, NormC, NormD, NormA, NormB)
+end subroutine auto2e_frontend_Spher_4_3_5_2
+end module auto2e_eri_hdgf

@@ -1,0 +1,150 @@
+!
+! Compute a batch of two-electron repulsion integrals, (AB|CD), in the Cartesian Gaussian
+! and real spherical harmonic basis.
+! Angular momenta: A=1, B=0, C=1, and D=0
+!
+! The order of the angular-dependent prefactors (x-Ra(1))**lx*(y-Ra(2))**ly*(z-Ra(3))**lz
+! is defined by the following loop:
+! I = 1
+! for lx in A..0
+!     for ly in A-lx..0
+!         lz = A-lx-ly
+!         Index[(lx,ly,lz)] = I
+!         I = I + 1
+!
+! The contracted Gaussian functions are defined as
+!
+! PhiA(lx,ly,lz) = NormA(Index[(lx,ly,lz)]) * (x-Ra(1))**lx * (y-Ra(2))**ly * (z-Ra(3))**lz * 
+!     Sum(Ga=1..NprimA) CntrA(Ga) Exp(-ExpA(Ga) * ((x-Ra(1))**2 + (y-Ra(2))**2 + (z-Ra(3))**2))
+!
+! Kappa specifies the form of the interaction potential:
+! Kappa=0 for the Coulomb interaction operator 1/r12
+! Kappa=1/Omega**2 for the screened interaction potential Erf(Omega*r12)/r12
+!
+! Code generated automatically.
+!
+module auto2e_eri_psps
+use arithmetic
+use auto2e_KetTransfer
+use auto2e_SpherTransf
+use auto2e_WMatrix_part1
+use auto2e_WMatrix_part2
+use auto2e_WMatrix_part3
+implicit none
+
+contains
+
+subroutine auto2e_eri_1_0_1_0(G, Ra, CntrA, ExpA, NprimA, &
+Rb, CntrB, ExpB, NprimB, Rc, CntrC, ExpC, NprimC, &
+Rd, CntrD, ExpD, NprimD, Kappa)
+!
+! Two-electron integrals class: (ps|ps)
+! L-dependent normalization constants are not applied.
+! Output memory layout: ABCD
+!
+real(F64), dimension(3, *), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, ExpA, CntrB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, ExpC, CntrD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+G(1:3, 1:3) = ZERO
+call auto2e_W_1_1(G(1:3, 1:3), Ra, CntrA, ExpA, NprimA, Rb, CntrB, ExpB, NprimB, &
+Rc, CntrC, ExpC, NprimC, Rd, CntrD, ExpD, NprimD, Kappa, 1, 1)
+end subroutine auto2e_eri_1_0_1_0
+
+
+
+subroutine auto2e_Normalize_1_0_1_0_CDAB(Gcdab, Gabcd, NormA, NormB, NormC, NormD)
+!
+! Apply L-dependent normalization constants and change the memory layout:
+!
+! Input memory layout: ABCD
+! Output memory layout: CDAB
+!
+real(F64), dimension(*), intent(out) :: Gcdab
+real(F64), dimension(*), intent(in) :: Gabcd
+real(F64), dimension(*), intent(in) :: NormA, NormB, NormC, NormD
+integer :: a, b, c, d, v, w
+v = 1
+do d = 1, 1
+do c = 1, 3
+do b = 1, 1
+do a = 1, 3
+w = c + (d-1)*3 + (a-1)*3 + (b-1)*9
+Gcdab(w) = NormA(a)*NormB(b)*NormC(c)*NormD(d)*Gabcd(v)
+v = v + 1
+end do
+end do
+end do
+end do
+end subroutine auto2e_Normalize_1_0_1_0_CDAB
+
+subroutine auto2e_frontend_0_1_0_1(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(9) :: H
+call auto2e_eri_1_0_1_0(H, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_1_0_1_0_CDAB(G, H, NormB, NormA, NormD, NormC)
+end subroutine auto2e_frontend_0_1_0_1
+
+subroutine auto2e_frontend_1_0_0_1(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(9) :: H
+call auto2e_eri_1_0_1_0(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rd, CntrD, ExpD, NprimD, &
+   Rc, CntrC, ExpC, NprimC, Kappa)
+call auto2e_Normalize_1_0_1_0_CDAB(G, H, NormA, NormB, NormD, NormC)
+end subroutine auto2e_frontend_1_0_0_1
+
+subroutine auto2e_frontend_0_1_1_0(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(9) :: H
+call auto2e_eri_1_0_1_0(H, Rb, CntrB, ExpB, NprimB, &
+   Ra, CntrA, ExpA, NprimA, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_1_0_1_0_CDAB(G, H, NormB, NormA, NormC, NormD)
+end subroutine auto2e_frontend_0_1_1_0
+
+subroutine auto2e_frontend_1_0_1_0(G, Ra, CntrA, NormA, ExpA, NprimA, &
+Rb, CntrB, NormB, ExpB, NprimB, Rc, CntrC, NormC, ExpC, NprimC, &
+Rd, CntrD, NormD, ExpD, NprimD, Kappa)
+real(F64), dimension(*), intent(out) :: G
+real(F64), dimension(3), intent(in) :: Ra, Rb, Rc, Rd
+real(F64), dimension(*), intent(in) :: CntrA, NormA, ExpA, CntrB, NormB, ExpB
+real(F64), dimension(*), intent(in) :: CntrC, NormC, ExpC, CntrD, NormD, ExpD
+integer, intent(in) :: NprimA, NprimB, NprimC, NprimD
+real(F64), intent(in) :: Kappa
+real(F64), dimension(9) :: H
+call auto2e_eri_1_0_1_0(H, Ra, CntrA, ExpA, NprimA, &
+   Rb, CntrB, ExpB, NprimB, &
+   Rc, CntrC, ExpC, NprimC, &
+   Rd, CntrD, ExpD, NprimD, Kappa)
+call auto2e_Normalize_1_0_1_0_CDAB(G, H, NormA, NormB, NormC, NormD)
+end subroutine auto2e_frontend_1_0_1_0
+end module auto2e_eri_psps
