@@ -686,7 +686,7 @@ static void step1(Handle& H)
     int64_t nchol = 0;
     bool converged = false, go = maxnchol > 0;
     int64_t nmacro = 0;
-    DVec<double> dM, dLB, dMbb, dDb, dLb, dpdmax, dLp, dLinv, dMp, dsegmax, dscal;
+    DVec<double> dM, dLB, dMbb, dDb, dLb, dpdmax, dLp, dsegmax, dscal;
     DVec<int> dpiv, dnpiv;
     DVec<int64_t> dgidx, dsegloc, dbrow;
     DVec<int> dsegdim;
@@ -846,15 +846,20 @@ static void step1(Handle& H)
                     Lst2.release();
                     cap = ncap;
                 }
-                // vectors over all candidates: L_new = M(:, piv) Lp^{-T}
+                // vectors over all candidates: L_new Lp^T = M(:, piv), solved by forward
+                // substitution (the column-by-column recursion of chol2_Lj,
+                // Step1.f90:859-881, which stays backward stable when the batch
+                // holds nearly dependent pivots; an explicit inverse does not)
                 dLp.ensure((size_t)npiv * npiv);
-                dLinv.ensure((size_t)npiv * npiv);
                 CU(launch_gather_pivrows(dLb.p, (int)nbatch, dpiv.p, npiv, dLp.p, s));
-                CU(launch_tri_inv_lower(dLp.p, npiv, dLinv.p, s));
-                dMp.ensure((size_t)ncand * npiv);
-                CU(launch_gather_cols(dM.p, ncand, dpiv.p, ncand, npiv, dMp.p, ncand, s));
-                gemm_nt(C.blas, ncand, npiv, npiv, 1.0, dMp.p, ncand, dLinv.p, npiv, 0.0, Lst.p + ncand * nchol, ncand);
-                H.gemm_flops[kGemmLnew] += 2.0 * ncand * npiv * npiv + (double)npiv * npiv * npiv / 3.0;
+                double* Lnew = Lst.p + ncand * nchol;
+                CU(launch_gather_cols(dM.p, ncand, dpiv.p, ncand, npiv, Lnew, ncand, s));
+                {
+                    const double one = 1.0;
+                    CB(cublasDtrsm_64(C.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                                      CUBLAS_DIAG_NON_UNIT, ncand, npiv, &one, dLp.p, npiv, Lnew, ncand));
+                }
+                H.gemm_flops[kGemmLnew] += (double)ncand * npiv * npiv;
                 CU(launch_downdate(dD.p, Lst.p + ncand * nchol, ncand, ncand, npiv, s));
             }
             T.stop();

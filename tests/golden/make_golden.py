@@ -12,7 +12,9 @@ Python code (run in a container that has the reference source mounted).
 Usage: python tests/golden/make_golden.py /path/to/reference
 """
 import json
+import os
 import sys
+import tempfile
 from pathlib import Path
 
 import numpy as np
@@ -23,9 +25,14 @@ HERE = Path(__file__).resolve().parent
 def main(ref_root: str) -> None:
     auto2e = Path(ref_root) / "src" / "integrals" / "Auto2e"
     sys.path.insert(0, str(auto2e))
+    # importing the generator writes its Fortran output under ./src; keep that
+    # out of this tree by importing from a scratch directory
+    here = os.getcwd()
+    os.chdir(tempfile.mkdtemp(prefix="auto2e_gen_"))
     import Auto2eGlobal as G        # noqa: E402  (reference module)
     import AutoSpherTransf as AST   # noqa: E402  (reference module)
     import Auto2e as A2E            # noqa: E402  (reference module: tuvindices)
+    os.chdir(here)
 
     U = {}
     for L in range(0, 6):
