@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -341,16 +342,15 @@ struct Handle {
 static constexpr double kPrimRel = 1.0e-17;
 static constexpr double kPrimAbs = 1.0e-22;
 
-static void setup_pairs(Handle& H)
+// Host half of the pair table: every shell pair A >= B in the Vdiag order with
+// its orientation, kept primitive pairs (plist) and record offsets; `rec` is
+// the total size of the primitive-pair records in doubles.
+static void build_pair_table(const HostBasis& b, PairTable& P, std::vector<int>& plist, int64_t& rec_total)
 {
-    Context& C = ctx();
-    const HostBasis& b = H.hb;
-    PairTable& P = H.pt;
     const int nsh = b.nsh;
     P.n = (int64_t)nsh * (nsh + 1) / 2;
     P.A.resize(P.n); P.B.resize(P.n); P.type.resize(P.n); P.dim.resize(P.n); P.nab.resize(P.n);
     P.vdloc.resize(P.n); P.h.resize(P.n);
-    std::vector<int> plist;
     std::vector<double> w;
     std::vector<double> minexp(nsh, 1e300);
     for (int s = 0; s < nsh; ++s)
@@ -413,6 +413,17 @@ static void setup_pairs(Handle& H)
             P.h[sp] = d;
             ++sp;
         }
+    rec_total = rec;
+}
+
+static void setup_pairs(Handle& H)
+{
+    Context& C = ctx();
+    const HostBasis& b = H.hb;
+    PairTable& P = H.pt;
+    std::vector<int> plist;
+    int64_t rec = 0;
+    build_pair_table(b, P, plist, rec);
     DevBasis& D = H.db;
     D.xyz.upload(b.xyz, C.stream);
     D.exps.upload(b.exps, C.stream);
@@ -1163,6 +1174,49 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
     T.flush();
 }
 
+// ------------------------------------------------------------------ allocation-free ERI matrix
+// The one scratch of gci_eri_pairs_noalloc.  It is static device storage of
+// the library's module, so every GPU on which that module is loaded holds
+// these bytes until the process exits; nothing is allocated per call.  In
+// host code `g_noalloc_scratch` only names the symbol -- its device address
+// on a device comes from cudaGetSymbolAddress with that device current.
+constexpr size_t kNoAllocScratchBytes = (size_t)GCI_NOALLOC_SCRATCH_BYTES;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mutex;
+static unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch on device `dev` (the current device), looked
+// up on the first call for that device and kept for the process.
+static unsigned char* noalloc_scratch(int dev)
+{
+    if (dev < 0 || dev >= kNoAllocMaxDevices) fail(GCI_ERR_ARG, "device ordinal beyond the no-alloc scratch table");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            fail(GCI_ERR_CUDA, std::string("cudaGetSymbolAddress of the no-alloc scratch failed: ") +
+                                   cudaGetErrorString(e));
+        }
+        g_noalloc_addr[dev] = (unsigned char*)p;
+    }
+    return g_noalloc_addr[dev];
+}
+
+// Byte offsets of the pieces placed in the scratch, each on a 256-byte boundary.
+struct ScratchPlan {
+    size_t end = 0;
+    size_t take(size_t bytes)
+    {
+        const size_t at = end;
+        end += (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+        return at;
+    }
+};
+
 } // namespace gci
 
 // =================================================================== C ABI
@@ -1413,6 +1467,111 @@ int gci_eri_pairs(const gci_basis* basis, double omega, double* out, int64_t ld)
         run_eri(H, all, all, kModeProduct, &m, &m, d.p, ld);
         CU(cudaMemcpyAsync(out, d.p, sizeof(double) * ld * npq, cudaMemcpyDeviceToHost, C.stream));
         CU(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int gci_eri_pairs_noalloc(const gci_basis* basis, double omega, double* out_dev, int64_t ld, void* stream)
+{
+    if (!out_dev) { g_last_error = "out_dev is NULL"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        const cudaStream_t s = (cudaStream_t)stream;
+        // host tables: the same basis, pair table and index maps as gci_eri_pairs
+        const HostBasis hb = make_basis(basis);
+        PairTable P;
+        std::vector<int> plist;
+        int64_t nrec = 0;
+        build_pair_table(hb, P, plist, nrec);
+        if (plist.empty()) plist.push_back(0);
+        int64_t npq = 0;
+        for (int64_t i = 0; i < P.n; ++i) npq += P.dim[i];
+        if (ld < npq) fail(GCI_ERR_ARG, "leading dimension too small");
+        std::vector<int64_t> moff(P.n);
+        std::vector<int> mmap;
+        for (int64_t sp = 0; sp < P.n; ++sp) {
+            const int A = P.A[sp], B = P.B[sp], Na = hb.nfunc[A], Nb = hb.nfunc[B];
+            moff[sp] = (int64_t)mmap.size();
+            for (int bb = 0; bb < Nb; ++bb)
+                for (int a = 0; a < Na; ++a) {
+                    const int64_t l = pair_local(a, bb, Na, A == B);
+                    mmap.push_back(l < 0 ? -1 : (int)(P.vdloc[sp] + l));
+                }
+        }
+        // pair ids grouped by pair type (one kernel per class of type pair)
+        std::vector<int64_t> seg(kNumPairTypes + 1, 0);
+        for (int64_t sp = 0; sp < P.n; ++sp) seg[P.type[sp] + 1]++;
+        for (int t = 0; t < kNumPairTypes; ++t) seg[t + 1] += seg[t];
+        std::vector<int> ids(P.n);
+        {
+            std::vector<int64_t> pos(seg.begin(), seg.end() - 1);
+            for (int64_t sp = 0; sp < P.n; ++sp) ids[pos[P.type[sp]]++] = (int)sp;
+        }
+        const std::vector<double> boys = boys_table(kBoysMaxM);
+
+        // scratch layout; reject before touching the device if it does not fit
+        ScratchPlan L;
+        auto bytes = [](const auto& v) { return v.size() * sizeof(v[0]); };
+        const size_t o_err = L.take(sizeof(int)), o_boys = L.take(bytes(boys));
+        const size_t o_xyz = L.take(bytes(hb.xyz)), o_exps = L.take(bytes(hb.exps)), o_coefs = L.take(bytes(hb.coefs));
+        const size_t o_tmat = L.take(bytes(hb.tmat)), o_poff = L.take(bytes(hb.poff));
+        const size_t o_nfunc = L.take(bytes(hb.nfunc)), o_loc = L.take(bytes(hb.loc)), o_toff = L.take(bytes(hb.toff));
+        const size_t o_pairs = L.take(bytes(P.h)), o_plist = L.take(bytes(plist));
+        const size_t o_pp = L.take(sizeof(double) * (size_t)std::max<int64_t>(nrec, 1));
+        const size_t o_moff = L.take(bytes(moff)), o_mmap = L.take(bytes(mmap)), o_ids = L.take(bytes(ids));
+        if (L.end > kNoAllocScratchBytes)
+            fail(GCI_ERR_BUFFER, "basis needs " + std::to_string(L.end) + " bytes of scratch; gci_eri_pairs_noalloc holds " +
+                                     std::to_string(kNoAllocScratchBytes) + " (use gci_eri_pairs for this basis)");
+
+        int dev = 0;
+        CU(cudaGetDevice(&dev));
+        unsigned char* base = noalloc_scratch(dev);
+        CU(eri_module_init());
+        // every piece below is rewritten on each call; the error word is cleared
+        auto put = [&](size_t off, const auto& v) {
+            if (!v.empty()) CU(cudaMemcpyAsync(base + off, v.data(), bytes(v), cudaMemcpyHostToDevice, s));
+        };
+        CU(cudaMemsetAsync(base + o_err, 0, sizeof(int), s));
+        put(o_boys, boys);
+        put(o_xyz, hb.xyz); put(o_exps, hb.exps); put(o_coefs, hb.coefs); put(o_tmat, hb.tmat);
+        put(o_poff, hb.poff); put(o_nfunc, hb.nfunc); put(o_loc, hb.loc); put(o_toff, hb.toff);
+        put(o_pairs, P.h); put(o_plist, plist); put(o_moff, moff); put(o_mmap, mmap); put(o_ids, ids);
+        CU(cudaMemsetAsync(out_dev, 0, sizeof(double) * (size_t)ld * npq, s));
+        auto dp = [&](size_t off) { return (double*)(base + off); };
+        auto ip = [&](size_t off) { return (int*)(base + off); };
+        const ShellPairDev* dpairs = (const ShellPairDev*)(base + o_pairs);
+        CU(pair_records_launch(dpairs, (int)P.n, dp(o_xyz), ip(o_poff), dp(o_exps), dp(o_coefs), ip(o_plist),
+                               dp(o_pp), s));
+        EriArgs a{};
+        a.sh_xyz = dp(o_xyz);
+        a.sh_toff = ip(o_toff);
+        a.tmat = dp(o_tmat);
+        a.sh_nfunc = ip(o_nfunc);
+        a.sh_loc = ip(o_loc);
+        a.pairs = dpairs;
+        a.pp = dp(o_pp);
+        a.mode = kModeProduct;
+        a.out = out_dev;
+        a.ldo = ld;
+        a.row_off = a.col_off = (const int64_t*)(base + o_moff);
+        a.row_map = a.col_map = ip(o_mmap);
+        a.nao = hb.nao;
+        a.kappa = (omega > 0.0) ? 1.0 / (omega * omega) : 0.0;
+        a.boys = dp(o_boys);
+        a.err = ip(o_err);
+        for (int tb = 0; tb < kNumPairTypes; ++tb)
+            for (int tk = 0; tk < kNumPairTypes; ++tk) {
+                const int64_t nb = seg[tb + 1] - seg[tb], nk = seg[tk + 1] - seg[tk];
+                if (nb == 0 || nk == 0) continue;
+                a.bra_ids = ip(o_ids) + seg[tb];
+                a.ket_ids = ip(o_ids) + seg[tk];
+                a.nbra = nb;
+                a.nket = nk;
+                a.swap_bk = tb < tk ? 1 : 0;
+                CU(eri_launch(std::max(tb, tk), std::min(tb, tk), a, s));
+            }
+        int herr = 0;
+        CU(cudaMemcpyAsync(&herr, base + o_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (herr != 0) fail(GCI_ERR_CUDA, "ERI kernel reported error " + std::to_string(herr));
     });
 }
 

@@ -158,6 +158,37 @@ int gci_normalize_basis(int64_t nparams, int64_t ldprim, const int64_t *L, const
  * triangle for ShA == ShB).  Small bases only (tests). */
 int gci_eri_pairs(const gci_basis *basis, double omega, double *out, int64_t ld);
 
+/* ---- allocation-free entry point (no counterpart in the reference) ---- */
+
+/* Size of the fixed device scratch behind gci_eri_pairs_noalloc: a file-scope
+ * __device__ array that every GPU on which libgci.so's code is loaded holds
+ * until the process exits. */
+#define GCI_NOALLOC_SCRATCH_BYTES ((int64_t)16 << 20)
+
+/* The same NPQ x NPQ ERI matrix as gci_eri_pairs, for callers that cannot
+ * allocate device memory: host codes whose device memory is owned by another
+ * allocator (a caching pool that has reserved the card, e.g. a framework's or a
+ * Fortran host program's), and code paths that must not call cudaMalloc or
+ * cudaFree because those calls synchronise the whole device.  This call makes
+ * no cudaMalloc or cudaFree call and uses no allocating library routine; its
+ * working data (Boys table, basis, shell-pair tables, primitive-pair records,
+ * index maps) lives in the fixed scratch of GCI_NOALLOC_SCRATCH_BYTES.
+ *
+ *   out_dev  DEVICE pointer to ld x NPQ doubles (column-major), on the current
+ *            device; every element of the NPQ columns is written (rows past NPQ
+ *            are set to zero), orbital pairs in the gci_eri_pairs order.
+ *   stream   cudaStream_t to work on (NULL: the legacy default stream).  The
+ *            call returns after the stream has finished the work.
+ *
+ * A basis whose tables need more than GCI_NOALLOC_SCRATCH_BYTES is rejected
+ * with GCI_ERR_BUFFER before any device work (use gci_eri_pairs for it).
+ * The first call on a device looks up the scratch's device address on that
+ * device (once per device, with it current); make that first call before any
+ * stream capture.  All calls share the one scratch array, which keeps the last
+ * call's contents: calls that overlap on the GPU (other threads, other streams
+ * of the same device) race on it and must be serialised by the caller. */
+int gci_eri_pairs_noalloc(const gci_basis *basis, double omega, double *out_dev, int64_t ld, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,3 +37,18 @@ def test_normalisation_matches_oracle():
         np.testing.assert_allclose(tb.CntrCoeffs[:tb.NPrimitives[s], s],
                                    ob.coefs[ob.prim_off[s]:ob.prim_off[s] + ob.nprim[s]], rtol=1e-13)
     assert tb.NAOSpher == ob.nao
+
+
+def test_noalloc_rejects_oversized_basis_before_device_work():
+    # 8 f shells of 40 primitives on one centre need ~42 MB of pair records,
+    # beyond the fixed scratch; the size check comes before any CUDA call, so
+    # this runs without a GPU (the output pointer is never dereferenced)
+    import ctypes as C
+    mol = molecules.random_molecule(77, 1, 4.0, (3,) * 8, (40, 40), (0.1, 1e3))
+    tb = gbasis.from_molecule(mol)
+    s = tb.c_struct()
+    npq = tb.NAO * (tb.NAO + 1) // 2
+    rc = _capi.lib().gci_eri_pairs_noalloc(C.byref(s), 0.0, C.c_void_p(256), npq, None)
+    assert rc == _capi.GCI_ERR_BUFFER
+    msg = _capi.lib().gci_last_error().decode()
+    assert "scratch" in msg and str(_capi.GCI_NOALLOC_SCRATCH_BYTES) in msg
