@@ -1,23 +1,27 @@
 // eri_engine.cuh -- class-templated McMurchie-Davidson ERI kernel for sm_100a.
 //
 // One team of TW threads evaluates one contracted shell quartet (AB|CD) of a
-// canonical class (LA>=LB, LC>=LD, bra type >= ket type).  The arithmetic is
-// the reference's (src/integrals/Auto2e): the (LS|KS) matrix
-//   W(e,f) = sum_prims E^e_tuv (-1)^{tau+nu+phi} E^f R_{t+tau,u+nu,v+phi}
-// with single-centre Hermite coefficients (auto2e_WMatrix_part1.f90:743-812),
-// then the horizontal recurrence to (ab|cd) (auto2e_KetTransfer.f90) and the
-// Cartesian -> spherical / normalisation transforms (auto2e_SpherTransf.f90,
-// auto2e_Normalize_*).  The sums are reordered for the GPU:
+// canonical class (LA>=LB, LC>=LD, bra type >= ket type).  The integral is the
+// reference's (src/integrals/Auto2e) Hermite-Coulomb sum
+//   (ab|cd) = sum_prims E^{ab}_tuv (-1)^{tau+nu+phi} E^{cd}_{tau nu phi} R_{t+tau,u+nu,v+phi}
+// followed by the Cartesian -> spherical / normalisation transforms
+// (auto2e_SpherTransf.f90, auto2e_Normalize_*).  Unlike the reference, which
+// contracts single-centre (e0|f0) and then applies the horizontal recurrence
+// (auto2e_KetTransfer.f90), the bra and ket use two-centre coefficients E^{ab}
+// per primitive pair: the recurrence after contraction cancels
+// catastrophically when a contracted shell mixes tight and diffuse primitives
+// on distant centres (all digits of (ff|ff) lost for exponents in
+// [0.05, 5e3] 4.6 bohr apart), while the two-centre coefficients carry no
+// such cancellation.  The sums are reordered for the GPU:
 //
 //  * for each ket primitive pair k, the bra side is contracted over all bra
 //    primitive pairs i in Hermite space first:
-//        T(e, g) = sum_i sum_{h in supp(e)} Eb_i(e, h) R_ik(h + g)
+//        T(ab, g) = sum_i sum_{h in supp(ab)} Eb_i(ab, h) R_ik(h + g)
 //    with lane g of the team owning the ket Hermite index g = (tau,nu,phi)
-//    and T(e, g) for every bra function e in registers;
-//  * the ket transform W(e, f) += sum_g (-1)^|g| Ek_k(f, g) T(e, g) then runs
-//    once per ket primitive pair instead of once per primitive quartet;
-//  * the HRR uses its closed binomial form (a,b| = sum_k C(b,k)(A-B)^{b-k}(a+k,0|,
-//    so every output element of the epilogue is independent.
+//    and T(ab, g) for every bra Cartesian pair in registers;
+//  * the ket transform W(ab, cd) += sum_g (-1)^|g| Ek_k(cd, g) T(ab, g) then
+//    runs once per ket primitive pair instead of once per primitive quartet;
+//  * the epilogue applies the four one-index transforms and scatters.
 //
 // R_tuv (Helgaker 9.9.18-20), the bra coefficient products and W live in
 // shared memory; all index tables are built in shared memory once per block.
@@ -36,36 +40,44 @@ GCI_HD constexpr int herm_level(int h) { int n = 0; while (herm_n(n) <= h) ++n; 
 GCI_HD constexpr int herm_v(int h) { int n = herm_level(h), p = h - (n > 0 ? herm_n(n - 1) : 0), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return p - s * (s + 1) / 2; }
 GCI_HD constexpr int herm_u(int h) { int n = herm_level(h), p = h - (n > 0 ? herm_n(n - 1) : 0), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return s - (p - s * (s + 1) / 2); }
 GCI_HD constexpr int herm_t(int h) { return herm_level(h) - herm_u(h) - herm_v(h); }
-GCI_HD constexpr int supp_size(int g) { return (cart_x(g) + 1) * (cart_y(g) + 1) * (cart_z(g) + 1); }
 GCI_HD constexpr int cmax(int a, int b) { return a > b ? a : b; }
-GCI_HD constexpr double c_binom(int n, int k)
+
+// Cartesian pair e = (a, b) of shells (la, lb), b fastest: its Hermite extent
+// along each axis and the offset of its coefficient block in a per-axis table.
+GCI_HD constexpr int pair_ga(int la, int lb, int e) { return cart_off(la) + e / ncart(lb); }
+GCI_HD constexpr int pair_gb(int la, int lb, int e) { return cart_off(lb) + e % ncart(lb); }
+GCI_HD constexpr int pair_x(int la, int lb, int e) { return cart_x(pair_ga(la, lb, e)) + cart_x(pair_gb(la, lb, e)); }
+GCI_HD constexpr int pair_y(int la, int lb, int e) { return cart_y(pair_ga(la, lb, e)) + cart_y(pair_gb(la, lb, e)); }
+GCI_HD constexpr int pair_z(int la, int lb, int e) { return cart_z(pair_ga(la, lb, e)) + cart_z(pair_gb(la, lb, e)); }
+GCI_HD constexpr int pair_ox(int la, int lb, int e) { return e2_off(la, cart_x(pair_ga(la, lb, e)), cart_x(pair_gb(la, lb, e))); }
+GCI_HD constexpr int pair_oy(int la, int lb, int e) { return e2_off(la, cart_y(pair_ga(la, lb, e)), cart_y(pair_gb(la, lb, e))); }
+GCI_HD constexpr int pair_oz(int la, int lb, int e) { return e2_off(la, cart_z(pair_ga(la, lb, e)), cart_z(pair_gb(la, lb, e))); }
+GCI_HD constexpr int pair_supp(int la, int lb, int e)
 {
-    double b = 1.0;
-    for (int i = 0; i < k; ++i) b = b * (n - i) / (i + 1);
-    return b;
+    return (pair_x(la, lb, e) + 1) * (pair_y(la, lb, e) + 1) * (pair_z(la, lb, e) + 1);
 }
 
 template <int LA, int LB, int LC, int LD>
 struct EriShape {
     static constexpr int L1 = LA + LB, L2 = LC + LD, LT = L1 + L2;
-    static constexpr int E0 = cart_off(LA), NE = cart_off(L1 + 1) - E0;
-    static constexpr int F0 = cart_off(LC), NF = cart_off(L2 + 1) - F0;
-    static constexpr int HT = herm_n(LT), H1 = herm_n(L1), H2 = herm_n(L2);
     static constexpr int nA = ncart(LA), nB = ncart(LB), nC = ncart(LC), nD = ncart(LD);
-    static constexpr int RSA = pp_record(L1), RSB = pp_record(L2);
+    static constexpr int NE = nA * nB, NF = nC * nD;     // bra (a,b) and ket (c,d) Cartesian pairs
+    static constexpr int HT = herm_n(LT), H1 = herm_n(L1), H2 = herm_n(L2);
+    static constexpr int EA = e2_size(LA, LB), EC = e2_size(LC, LD);   // per-axis coefficient tables
+    static constexpr int RSA = pp_record(LA, LB), RSB = pp_record(LC, LD);
     static constexpr int cb_count()
     {
         int n = 0;
-        for (int e = 0; e < NE; ++e) n += supp_size(E0 + e);
+        for (int e = 0; e < NE; ++e) n += pair_supp(LA, LB, e);
         return n;
     }
     static constexpr int NCB = cb_count();
     // team scratch (doubles): W, R ping-pong, bra products, T spill
     static constexpr int O_W = 0, O_RA = NE * NF, O_RB = O_RA + HT, O_CB = O_RB + HT, O_TT = O_CB + NCB;
     static constexpr int SZ_MAIN = O_TT + NE * H2;
-    // epilogue ping-pong over the same scratch (P0 holds W on entry)
-    static constexpr int SZ_P0 = cmax(NE * NF, cmax(NE * nC * nD, nA * nB * nC * nD));
-    static constexpr int SZ_P1 = cmax(NE * nC * nD, nA * nB * nC * nD);
+    // epilogue ping-pong over the same scratch (P0 holds W on entry); every
+    // stage has at most NE * NF elements (spherical counts <= Cartesian)
+    static constexpr int SZ_P0 = NE * NF, SZ_P1 = NE * NF;
     static constexpr int SZ_TEAM = cmax(SZ_MAIN, SZ_P0 + SZ_P1);
     // per-block tables (ints)
     static constexpr int TAB_CB = NCB;            // packed E-table offsets of each bra product
@@ -127,13 +139,11 @@ k_eri_class(const EriArgs a)
     // ---- per-block tables
     for (int c = threadIdx.x; c < S::NCB; c += TPB) {
         int e = 0, off = 0;
-        while (off + supp_size(S::E0 + e) <= c) { off += supp_size(S::E0 + e); ++e; }
-        const int g = S::E0 + e;
-        const int ex = cart_x(g), ey = cart_y(g);
+        while (off + pair_supp(LA, LB, e) <= c) { off += pair_supp(LA, LB, e); ++e; }
+        const int ex = pair_x(LA, LB, e), ey = pair_y(LA, LB, e);
         const int r = c - off;                       // order: v outer, u, t inner
         const int t = r % (ex + 1), u = (r / (ex + 1)) % (ey + 1), v = r / ((ex + 1) * (ey + 1));
-        const int ez = cart_z(g);
-        tab_cb[c] = (ex * (ex + 1) / 2 + t) | ((ey * (ey + 1) / 2 + u) << 8) | ((ez * (ez + 1) / 2 + v) << 16);
+        tab_cb[c] = (pair_ox(LA, LB, e) + t) | ((pair_oy(LA, LB, e) + u) << 8) | ((pair_oz(LA, LB, e) + v) << 16);
     }
     for (int c = threadIdx.x; c < S::TAB_RIDX; c += TPB) {
         const int g = c / S::H1, h = c - g * S::H1;
@@ -205,8 +215,8 @@ k_eri_class(const EriArgs a)
                 // bra coefficient products Eb(e,h) = Ex Ey Ez (this bra primitive pair)
                 {
                     const double* __restrict__ Ebx = Bp + 8;
-                    const double* __restrict__ Eby = Ebx + tri(S::L1);
-                    const double* __restrict__ Ebz = Eby + tri(S::L1);
+                    const double* __restrict__ Eby = Ebx + S::EA;
+                    const double* __restrict__ Ebz = Eby + S::EA;
                     for (int c = lane; c < S::NCB; c += TW) {
                         const int o = tab_cb[c];
                         CBv[c] = __ldg(Ebx + (o & 0xff)) * __ldg(Eby + ((o >> 8) & 0xff)) * __ldg(Ebz + (o >> 16));
@@ -250,14 +260,13 @@ k_eri_class(const EriArgs a)
                         int c = 0;
 #pragma unroll
                         for (int e = 0; e < S::NE; ++e) {
-                            const int g = S::E0 + e;
                             double acc = T[e];
 #pragma unroll
-                            for (int v = 0; v <= cart_z(g); ++v)
+                            for (int v = 0; v <= pair_z(LA, LB, e); ++v)
 #pragma unroll
-                                for (int u = 0; u <= cart_y(g); ++u)
+                                for (int u = 0; u <= pair_y(LA, LB, e); ++u)
 #pragma unroll
-                                    for (int t = 0; t <= cart_x(g); ++t) {
+                                    for (int t = 0; t <= pair_x(LA, LB, e); ++t) {
                                         acc += CBv[c] * Rl[herm_idx(t, u, v)];
                                         ++c;
                                     }
@@ -267,14 +276,13 @@ k_eri_class(const EriArgs a)
                         int c = 0;
 #pragma unroll
                         for (int e = 0; e < S::NE; ++e) {
-                            const int g = S::E0 + e;
                             double acc = T[e];
 #pragma unroll
-                            for (int v = 0; v <= cart_z(g); ++v)
+                            for (int v = 0; v <= pair_z(LA, LB, e); ++v)
 #pragma unroll
-                                for (int u = 0; u <= cart_y(g); ++u)
+                                for (int u = 0; u <= pair_y(LA, LB, e); ++u)
 #pragma unroll
-                                    for (int t = 0; t <= cart_x(g); ++t) {
+                                    for (int t = 0; t <= pair_x(LA, LB, e); ++t) {
                                         acc += CBv[c] * cur[ridx[herm_idx(t, u, v)]];
                                         ++c;
                                     }
@@ -293,20 +301,20 @@ k_eri_class(const EriArgs a)
             team_sync<TW, TPB>();
             {
                 const double* __restrict__ Ekx = K + 8;
-                const double* __restrict__ Eky = Ekx + tri(S::L2);
-                const double* __restrict__ Ekz = Eky + tri(S::L2);
+                const double* __restrict__ Eky = Ekx + S::EC;
+                const double* __restrict__ Ekz = Eky + S::EC;
                 for (int f = lane; f < S::NF; f += TW) {
-                    const int fg = S::F0 + f;
-                    const int fx = cart_x(fg), fy = cart_y(fg), fz = cart_z(fg);
+                    const int fx = pair_x(LC, LD, f), fy = pair_y(LC, LD, f), fz = pair_z(LC, LD, f);
+                    const int ox = pair_ox(LC, LD, f), oy = pair_oy(LC, LD, f), oz = pair_oz(LC, LD, f);
                     double wcol[S::NE];
 #pragma unroll
                     for (int e = 0; e < S::NE; ++e) wcol[e] = WW[e * S::NF + f];
                     for (int p3 = 0; p3 <= fz; ++p3) {
-                        const double cz = __ldg(Ekz + fz * (fz + 1) / 2 + p3) * ((p3 & 1) ? -1.0 : 1.0);
+                        const double cz = __ldg(Ekz + oz + p3) * ((p3 & 1) ? -1.0 : 1.0);
                         for (int p2 = 0; p2 <= fy; ++p2) {
-                            const double cyz = cz * __ldg(Eky + fy * (fy + 1) / 2 + p2) * ((p2 & 1) ? -1.0 : 1.0);
+                            const double cyz = cz * __ldg(Eky + oy + p2) * ((p2 & 1) ? -1.0 : 1.0);
                             for (int p1 = 0; p1 <= fx; ++p1) {
-                                const double c = cyz * __ldg(Ekx + fx * (fx + 1) / 2 + p1) * ((p1 & 1) ? -1.0 : 1.0);
+                                const double c = cyz * __ldg(Ekx + ox + p1) * ((p1 & 1) ? -1.0 : 1.0);
                                 const int g = herm_idx(p1, p2, p3);
 #pragma unroll
                                 for (int e = 0; e < S::NE; ++e) wcol[e] += c * TT[e * S::H2 + g];
@@ -320,94 +328,37 @@ k_eri_class(const EriArgs a)
             team_sync<TW, TPB>();
         }
 
-        // ================= epilogue: HRR + transforms + scatter =================
-        double* P0 = WW;                 // holds W(e, f) on entry
+        // ================= epilogue: transforms + scatter =================
+        double* P0 = WW;                 // holds W[ab][cd] on entry
         double* P1 = WW + S::SZ_P0;
         const int A = pb.s1, B = pb.s2, C = pk.s1, D = pk.s2;
-        const double ABx = __ldg(a.sh_xyz + 3 * A) - __ldg(a.sh_xyz + 3 * B);
-        const double ABy = __ldg(a.sh_xyz + 3 * A + 1) - __ldg(a.sh_xyz + 3 * B + 1);
-        const double ABz = __ldg(a.sh_xyz + 3 * A + 2) - __ldg(a.sh_xyz + 3 * B + 2);
-        const double CDx = __ldg(a.sh_xyz + 3 * C) - __ldg(a.sh_xyz + 3 * D);
-        const double CDy = __ldg(a.sh_xyz + 3 * C + 1) - __ldg(a.sh_xyz + 3 * D + 1);
-        const double CDz = __ldg(a.sh_xyz + 3 * C + 2) - __ldg(a.sh_xyz + 3 * D + 2);
         const int nfA = __ldg(a.sh_nfunc + A), nfB = __ldg(a.sh_nfunc + B);
         const int nfC = __ldg(a.sh_nfunc + C), nfD = __ldg(a.sh_nfunc + D);
-        // 1) ket HRR: X[e][c][d] (P1)
-        for (int idx = lane; idx < S::NE * S::nC * S::nD; idx += TW) {
-            const int e = idx / (S::nC * S::nD);
-            const int r = idx - e * (S::nC * S::nD);
-            const int c = r / S::nD, d = r - c * S::nD;
-            const int cg = cart_off(LC) + c, dg = cart_off(LD) + d;
-            const int cy = cart_y(cg), cz = cart_z(cg);
-            const int dx = cart_x(dg), dy = cart_y(dg), dz = cart_z(dg);
-            double acc = 0.0;
-            double pz = 1.0;
-            for (int kz = dz; kz >= 0; --kz) {
-                double py = 1.0;
-                for (int ky = dy; ky >= 0; --ky) {
-                    double px = 1.0;
-                    for (int kx = dx; kx >= 0; --kx) {
-                        const int fi = cart_off(LC + kx + ky + kz) + cart_pos(cy + ky, cz + kz) - S::F0;
-                        acc += c_binom(dx, kx) * c_binom(dy, ky) * c_binom(dz, kz) * px * py * pz * P0[e * S::NF + fi];
-                        px *= CDx;
-                    }
-                    py *= CDy;
-                }
-                pz *= CDz;
-            }
-            P1[idx] = acc;
-        }
-        team_sync<TW, TPB>();
-        // 2) T_D on d: U[e][c][md] (P0)
         const double* __restrict__ TA = a.tmat + __ldg(a.sh_toff + A);
         const double* __restrict__ TB = a.tmat + __ldg(a.sh_toff + B);
         const double* __restrict__ TC = a.tmat + __ldg(a.sh_toff + C);
         const double* __restrict__ TD = a.tmat + __ldg(a.sh_toff + D);
+        // 1) T_D on d: U[ab][c][md] (P1)
         for (int idx = lane; idx < S::NE * S::nC * nfD; idx += TW) {
             const int ec = idx / nfD, md = idx - ec * nfD;
             double acc = 0.0;
 #pragma unroll
-            for (int d = 0; d < S::nD; ++d) acc += __ldg(TD + md * S::nD + d) * P1[ec * S::nD + d];
-            P0[idx] = acc;
+            for (int d = 0; d < S::nD; ++d) acc += __ldg(TD + md * S::nD + d) * P0[ec * S::nD + d];
+            P1[idx] = acc;
         }
         team_sync<TW, TPB>();
-        // 3) T_C on c: Y[e][mc][md] (P1)
+        // 2) T_C on c: Y[ab][mc][md] (P0)
         const int nq = nfC * nfD;
         for (int idx = lane; idx < S::NE * nq; idx += TW) {
             const int e = idx / nq, q = idx - e * nq;
             const int mc = q / nfD, md = q - mc * nfD;
             double acc = 0.0;
 #pragma unroll
-            for (int c = 0; c < S::nC; ++c) acc += __ldg(TC + mc * S::nC + c) * P0[(e * S::nC + c) * nfD + md];
-            P1[idx] = acc;
-        }
-        team_sync<TW, TPB>();
-        // 4) bra HRR: Z[a][b][q] (P0)
-        for (int idx = lane; idx < S::nA * S::nB * nq; idx += TW) {
-            const int ab = idx / nq, q = idx - ab * nq;
-            const int ai = ab / S::nB, bi = ab - ai * S::nB;
-            const int ag = cart_off(LA) + ai, bg = cart_off(LB) + bi;
-            const int ay = cart_y(ag), az = cart_z(ag);
-            const int bx = cart_x(bg), by = cart_y(bg), bz = cart_z(bg);
-            double acc = 0.0;
-            double pz = 1.0;
-            for (int kz = bz; kz >= 0; --kz) {
-                double py = 1.0;
-                for (int ky = by; ky >= 0; --ky) {
-                    double px = 1.0;
-                    for (int kx = bx; kx >= 0; --kx) {
-                        const int ei = cart_off(LA + kx + ky + kz) + cart_pos(ay + ky, az + kz) - S::E0;
-                        acc += c_binom(bx, kx) * c_binom(by, ky) * c_binom(bz, kz) * px * py * pz * P1[ei * nq + q];
-                        px *= ABx;
-                    }
-                    py *= ABy;
-                }
-                pz *= ABz;
-            }
+            for (int c = 0; c < S::nC; ++c) acc += __ldg(TC + mc * S::nC + c) * P1[(e * S::nC + c) * nfD + md];
             P0[idx] = acc;
         }
         team_sync<TW, TPB>();
-        // 5) T_B on b: V1[a][mb][q] (P1)
+        // 3) T_B on b: V1[a][mb][q] (P1)
         for (int idx = lane; idx < S::nA * nfB * nq; idx += TW) {
             const int am = idx / nq, q = idx - am * nq;
             const int ai = am / nfB, mb = am - ai * nfB;
@@ -417,7 +368,7 @@ k_eri_class(const EriArgs a)
             P1[idx] = acc;
         }
         team_sync<TW, TPB>();
-        // 6) T_A on a and scatter
+        // 4) T_A on a and scatter
         const int nout = nfA * nfB * nq;
         for (int idx = lane; idx < nout; idx += TW) {
             const int mm = idx / nq, q = idx - mm * nq;

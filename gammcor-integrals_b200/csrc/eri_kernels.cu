@@ -7,7 +7,12 @@ namespace gci {
 
 // ---------------------------------------------------------------------------
 // Primitive-pair records (one block per shell pair, threads over primitive
-// pairs, a fastest as in the reference's Ga-inner loop).
+// pairs, a fastest as in the reference's Ga-inner loop).  The Hermite
+// coefficients are the two-centre E^{ij}_t of (x-A)^i (x-B)^j about P
+// (McMurchie-Davidson recursion in P-A and P-B), so the ERI kernels need no
+// horizontal recurrence: that recurrence, applied after the primitive
+// contraction, cancels catastrophically for contracted shells that mix tight
+// and diffuse primitives on distant centres.
 // ---------------------------------------------------------------------------
 __global__ void k_pair_records(const ShellPairDev* __restrict__ pairs, int npairs,
                                const double* __restrict__ xyz, const int* __restrict__ poff,
@@ -16,8 +21,9 @@ __global__ void k_pair_records(const ShellPairDev* __restrict__ pairs, int npair
 {
     for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
         const ShellPairDev sp = pairs[p];
-        const int L1 = sp.l1 + sp.l2;
-        const int rs = pp_record(L1);
+        const int la = sp.l1, lb = sp.l2;
+        const int rs = pp_record(la, lb);
+        const int ne = e2_size(la, lb);
         const int n = sp.npp;
         const double ax = xyz[3 * sp.s1], ay = xyz[3 * sp.s1 + 1], az = xyz[3 * sp.s1 + 2];
         const double bx = xyz[3 * sp.s2], by = xyz[3 * sp.s2 + 1], bz = xyz[3 * sp.s2 + 2];
@@ -33,23 +39,38 @@ __global__ void k_pair_records(const ShellPairDev* __restrict__ pairs, int npair
             rec[0] = P; rec[1] = px; rec[2] = py; rec[3] = pz;
             rec[4] = exp(-ea * eb / P * r2) * ca * cb;
             rec[5] = px - ax; rec[6] = py - ay; rec[7] = pz - az;
-            // single-centre Hermite coefficients E^{e}_t (auto2e_EtCoeffs_L)
             const double h = 1.0 / (2.0 * P);
+            const double PA[3] = {px - ax, py - ay, pz - az};
+            const double PB[3] = {px - bx, py - by, pz - bz};
             for (int axis = 0; axis < 3; ++axis) {
-                double* E = rec + 8 + axis * tri(L1);
-                const double X = rec[5 + axis];
+                double* E = rec + 8 + axis * ne;
                 E[0] = 1.0;
-                for (int e = 0; e < L1; ++e) {
-                    const double* Ee = E + e * (e + 1) / 2;
-                    double* En = E + (e + 1) * (e + 2) / 2;
-                    for (int t = 0; t <= e + 1; ++t) {
+                // raise i on A: E^{i+1,0}
+                for (int a = 0; a < la; ++a) {
+                    const double* Ei = E + e2_off(la, a, 0);
+                    double* En = E + e2_off(la, a + 1, 0);
+                    for (int t = 0; t <= a + 1; ++t) {
                         double v = 0.0;
-                        if (t >= 1) v += h * Ee[t - 1];
-                        if (t <= e) v += X * Ee[t];
-                        if (t + 1 <= e) v += (double)(t + 1) * Ee[t + 1];
+                        if (t >= 1) v += h * Ei[t - 1];
+                        if (t <= a) v += PA[axis] * Ei[t];
+                        if (t + 1 <= a) v += (double)(t + 1) * Ei[t + 1];
                         En[t] = v;
                     }
                 }
+                // raise j on B: E^{i,j+1}
+                for (int b = 0; b < lb; ++b)
+                    for (int a = 0; a <= la; ++a) {
+                        const double* Ej = E + e2_off(la, a, b);
+                        double* En = E + e2_off(la, a, b + 1);
+                        const int m = a + b;
+                        for (int t = 0; t <= m + 1; ++t) {
+                            double v = 0.0;
+                            if (t >= 1) v += h * Ej[t - 1];
+                            if (t <= m) v += PB[axis] * Ej[t];
+                            if (t + 1 <= m) v += (double)(t + 1) * Ej[t + 1];
+                            En[t] = v;
+                        }
+                    }
             }
         }
     }

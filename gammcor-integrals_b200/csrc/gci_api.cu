@@ -408,7 +408,7 @@ static void build_pair_table(const HostBasis& b, PairTable& P, std::vector<int>&
                 }
             d.npp = kept;
             d.rec_off = rec;
-            rec += (int64_t)kept * pp_record(d.l1 + d.l2);
+            rec += (int64_t)kept * pp_record(d.l1, d.l2);
             P.type[sp] = pair_type(d.l1, d.l2);
             P.h[sp] = d;
             ++sp;

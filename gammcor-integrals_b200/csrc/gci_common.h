@@ -36,9 +36,18 @@ GCI_HD constexpr int cart_pos(int ly, int lz) { return (ly + lz) * (ly + lz + 1)
 GCI_HD constexpr int pair_type(int lhi, int llo) { return lhi * (lhi + 1) / 2 + llo; }
 constexpr int kNumPairTypes = pair_type(kMaxL, kMaxL) + 1;
 
-// Size in doubles of one primitive-pair record of a pair whose level is L1:
-//   [0] P  [1..3] Rp  [4] K_ab c_a c_b  [5..7] Rp - A  [8..] E^{e}_t, x/y/z
-GCI_HD constexpr int pp_record(int l1) { return 8 + 3 * tri(l1); }
+// Two-centre Hermite coefficients E^{ij}_t of (x-A)^i (x-B)^j exp(-p (x-P)^2),
+// i <= la, j <= lb, t <= i+j, one table per axis: block (i, j) starts at
+// e2_off(la, i, j) (j major, then i), e2_size entries in all.
+GCI_HD constexpr int e2_off(int la, int i, int j)
+{
+    return (la + 1) * j * (j + 1) / 2 + j * la * (la + 1) / 2 + i * (j + 1) + i * (i - 1) / 2;
+}
+GCI_HD constexpr int e2_size(int la, int lb) { return (la + 1) * (lb + 1) * (la + lb + 2) / 2; }
+
+// Size in doubles of one primitive-pair record of a pair (l1, l2):
+//   [0] P  [1..3] Rp  [4] K_ab c_a c_b  [5..7] Rp - A  [8..] E^{ij}_t, x/y/z tables
+GCI_HD constexpr int pp_record(int l1, int l2) { return 8 + 3 * e2_size(l1, l2); }
 
 // Output modes of the ERI kernels.
 enum EriMode : int {

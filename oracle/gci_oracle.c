@@ -494,6 +494,177 @@ static void cart_quartet(int la, int lb, int lc, int ld,
     free(W); free(X); free(col); free(res);
 }
 
+/* ---------------------------------------------------------------------- */
+/* Two-centre Hermite form (no horizontal recurrence).                    */
+/*                                                                        */
+/* The W-matrix + HRR route above contracts (e0| on centre A over the     */
+/* primitive pairs and then moves angular momentum to B with              */
+/* (a,b| = sum_k C(b,k) (A-B)^{b-k} (a+k,0|.  For a primitive pair whose  */
+/* product centre P lies near B (tight primitive on B, diffuse one on A)  */
+/* that sum cancels ~ (|AB| sqrt(p))^{l_b}: for f shells contracted over  */
+/* [0.05, 5e3] on atoms 4.6 bohr apart the (ff|ff) quartet loses every    */
+/* digit (bra-ket symmetry broken by 33% of its largest element).  No     */
+/* single orientation of a contracted pair avoids it when both shells mix */
+/* tight and diffuse primitives.  The two-centre coefficients E^{ij}_t of */
+/* (x-A)^i (x-B)^j exp(-p(x-P)^2) (McMurchie-Davidson; Helgaker 9.5.6)    */
+/* are built per primitive pair from PA and PB without cancellation, and  */
+/*   (ab|cd) = sum E^{ab}_{tuv} (-1)^{tau+nu+phi} E^{cd}_{tau nu phi}     */
+/*             R_{t+tau,u+nu,v+phi}                                       */
+/* is the same integral.  The CUDA library evaluates this form; the       */
+/* W-matrix route stays here as the restatement of the reference.        */
+/* ---------------------------------------------------------------------- */
+
+/* offset of block (i, j), t = 0..i+j, in a per-axis table for i <= la, j major */
+static inline int e2_off(int la, int i, int j)
+{
+    return (la + 1) * j * (j + 1) / 2 + j * la * (la + 1) / 2 + i * (j + 1) + i * (i - 1) / 2;
+}
+static inline int e2_size(int la, int lb) { return (la + 1) * (lb + 1) * (la + lb + 2) / 2; }
+
+/* E^{ij}_t for i <= la, j <= lb (PA = P - A, PB = P - B along one axis) */
+static void e2_coeffs(int la, int lb, double p, double PA, double PB, double *E)
+{
+    const double h = 1.0 / (2.0 * p);
+    E[e2_off(la, 0, 0)] = 1.0;
+    for (int i = 0; i < la; ++i) {
+        const double *Ei = E + e2_off(la, i, 0);
+        double *En = E + e2_off(la, i + 1, 0);
+        for (int t = 0; t <= i + 1; ++t) {
+            double v = 0.0;
+            if (t >= 1) v += h * Ei[t - 1];
+            if (t <= i) v += PA * Ei[t];
+            if (t + 1 <= i) v += (t + 1) * Ei[t + 1];
+            En[t] = v;
+        }
+    }
+    for (int j = 0; j < lb; ++j)
+        for (int i = 0; i <= la; ++i) {
+            const double *Ej = E + e2_off(la, i, j);
+            double *En = E + e2_off(la, i, j + 1);
+            const int n = i + j;
+            for (int t = 0; t <= n + 1; ++t) {
+                double v = 0.0;
+                if (t >= 1) v += h * Ej[t - 1];
+                if (t <= n) v += PB * Ej[t];
+                if (t + 1 <= n) v += (t + 1) * Ej[t + 1];
+                En[t] = v;
+            }
+        }
+}
+
+static void cart_quartet_2c(int la, int lb, int lc, int ld,
+                            const double *Ra, const double *Rb, const double *Rc, const double *Rd,
+                            int na, const double *ea, const double *ca,
+                            int nb, const double *eb, const double *cb,
+                            int nc, const double *ec, const double *cc,
+                            int nd, const double *ed, const double *cd,
+                            double kappa, double *G)
+{
+    const int L1 = la + lb, L2 = lc + ld, LT = L1 + L2;
+    const int Na = NCART(la), Nb = NCART(lb), Nc = NCART(lc), Nd = NCART(ld);
+    const int a0 = CART_OFF(la), b0 = CART_OFF(lb), c0 = CART_OFF(lc), d0 = CART_OFF(ld);
+    const int sab = e2_size(la, lb), scd = e2_size(lc, ld);
+    memset(G, 0, sizeof(double) * (size_t)Na * Nb * Nc * Nd);
+    double Rab2 = 0, Rcd2 = 0;
+    for (int i = 0; i < 3; ++i) {
+        Rab2 += (Ra[i] - Rb[i]) * (Ra[i] - Rb[i]);
+        Rcd2 += (Rc[i] - Rd[i]) * (Rc[i] - Rd[i]);
+    }
+    double *Eab = (double *)malloc(sizeof(double) * 3 * sab);
+    double *Ecd = (double *)malloc(sizeof(double) * 3 * scd);
+    double *R = (double *)malloc(sizeof(double) * HERM_N(LT));
+    double *S = (double *)malloc(sizeof(double) * HERM_N(L1));
+    double F[MAXLT + 1];
+    for (int gd = 0; gd < nd; ++gd)
+        for (int gc = 0; gc < nc; ++gc) {
+            const double Q = ec[gc] + ed[gd];
+            const double mucd = ec[gc] * ed[gd] / Q;
+            double Rq[3];
+            for (int i = 0; i < 3; ++i) {
+                Rq[i] = (ec[gc] * Rc[i] + ed[gd] * Rd[i]) / Q;
+                e2_coeffs(lc, ld, Q, Rq[i] - Rc[i], Rq[i] - Rd[i], Ecd + i * scd);
+            }
+            for (int gb = 0; gb < nb; ++gb)
+                for (int ga = 0; ga < na; ++ga) {
+                    const double P = ea[ga] + eb[gb];
+                    const double muab = ea[ga] * eb[gb] / P;
+                    double Rp[3], Rpq[3];
+                    for (int i = 0; i < 3; ++i) {
+                        Rp[i] = (ea[ga] * Ra[i] + eb[gb] * Rb[i]) / P;
+                        Rpq[i] = Rp[i] - Rq[i];
+                        e2_coeffs(la, lb, P, Rp[i] - Ra[i], Rp[i] - Rb[i], Eab + i * sab);
+                    }
+                    const double kabcd = exp(-muab * Rab2 - mucd * Rcd2);
+                    const double PQ = P * Q;
+                    const double alpha = PQ / (P + Q + kappa * PQ);
+                    const double N = 2.0 * pow(PI, 2.5) / (PQ * sqrt(P + Q + kappa * PQ));
+                    const double e000 = N * ca[ga] * cb[gb] * cc[gc] * cd[gd] * kabcd;
+                    const double T = alpha * (Rpq[0] * Rpq[0] + Rpq[1] * Rpq[1] + Rpq[2] * Rpq[2]);
+                    orc_fm(LT, T, F);
+                    rtuv(LT, F, alpha, Rpq[0], Rpq[1], Rpq[2], R);
+                    for (int d = 0; d < Nd; ++d)
+                        for (int c = 0; c < Nc; ++c) {
+                            const int cx = g_cx[c0 + c], cy = g_cy[c0 + c], cz = g_cz[c0 + c];
+                            const int dx = g_cx[d0 + d], dy = g_cy[d0 + d], dz = g_cz[d0 + d];
+                            const double *Ex = Ecd + e2_off(lc, cx, dx);
+                            const double *Ey = Ecd + scd + e2_off(lc, cy, dy);
+                            const double *Ez = Ecd + 2 * scd + e2_off(lc, cz, dz);
+                            /* S(h) = sum_g (-1)^|g| E^{cd}_g R(h + g), h up to level L1 */
+                            for (int k = 0; k <= L1; ++k)
+                                for (int s = 0; s <= k; ++s)
+                                    for (int v = 0; v <= s; ++v) {
+                                        const int u = s - v, t = k - s;
+                                        double acc = 0.0;
+                                        for (int p3 = 0; p3 <= cz + dz; ++p3)
+                                            for (int p2 = 0; p2 <= cy + dy; ++p2)
+                                                for (int p1 = 0; p1 <= cx + dx; ++p1) {
+                                                    const double sg = ((p1 + p2 + p3) & 1) ? -1.0 : 1.0;
+                                                    acc += sg * Ex[p1] * Ey[p2] * Ez[p3] *
+                                                           R[herm_idx(t + p1, u + p2, v + p3)];
+                                                }
+                                        S[herm_idx(t, u, v)] = acc;
+                                    }
+                            const size_t q = (size_t)c + (size_t)Nc * d;
+                            for (int bi = 0; bi < Nb; ++bi)
+                                for (int ai = 0; ai < Na; ++ai) {
+                                    const int ax = g_cx[a0 + ai], ay = g_cy[a0 + ai], az = g_cz[a0 + ai];
+                                    const int bx = g_cx[b0 + bi], by = g_cy[b0 + bi], bz = g_cz[b0 + bi];
+                                    const double *Fx = Eab + e2_off(la, ax, bx);
+                                    const double *Fy = Eab + sab + e2_off(la, ay, by);
+                                    const double *Fz = Eab + 2 * sab + e2_off(la, az, bz);
+                                    double acc = 0.0;
+                                    for (int v = 0; v <= az + bz; ++v)
+                                        for (int u = 0; u <= ay + by; ++u)
+                                            for (int t = 0; t <= ax + bx; ++t)
+                                                acc += Fx[t] * Fy[u] * Fz[v] * S[herm_idx(t, u, v)];
+                                    G[(size_t)ai + (size_t)Na * bi + (size_t)Na * Nb * q] += e000 * acc;
+                                }
+                        }
+                }
+        }
+    free(Eab); free(Ecd); free(R); free(S);
+}
+
+/* Integral scheme of every quartet the oracle evaluates: 1 = two-centre
+ * Hermite form (what the CUDA library computes, default), 0 = the
+ * reference's W-matrix + HRR route. */
+static int g_eri_scheme = 1;
+void orc_set_eri_scheme(int scheme) { g_eri_scheme = scheme ? 1 : 0; }
+
+static void cart_quartet_any(int la, int lb, int lc, int ld,
+                             const double *Ra, const double *Rb, const double *Rc, const double *Rd,
+                             int na, const double *ea, const double *ca,
+                             int nb, const double *eb, const double *cb,
+                             int nc, const double *ec, const double *cc,
+                             int nd, const double *ed, const double *cd,
+                             double kappa, double *G)
+{
+    if (g_eri_scheme)
+        cart_quartet_2c(la, lb, lc, ld, Ra, Rb, Rc, Rd, na, ea, ca, nb, eb, cb, nc, ec, cc, nd, ed, cd, kappa, G);
+    else
+        cart_quartet(la, lb, lc, ld, Ra, Rb, Rc, Rd, na, ea, ca, nb, eb, cb, nc, ec, cc, nd, ed, cd, kappa, G);
+}
+
 /* Apply the per-shell transforms T (nfunc x ncart) to every index of a
  * 4-index block, a fastest (auto2e_SpherTransf.f90 + auto2e_Normalize_*). */
 static void transform4(const double *G, int n[4], const double *T[4], int nf[4], double *out)
@@ -588,7 +759,7 @@ int orc_eri_quartet(const orc_basis *b, int A, int B, int C, int D, double kappa
     size_t tot = (size_t)n[0] * n[1] * n[2] * n[3];
     double *Gc = (double *)malloc(sizeof(double) * tot);
     double *G = (double *)malloc(sizeof(double) * tot);
-    cart_quartet(cl[0], cl[1], cl[2], cl[3],
+    cart_quartet_any(cl[0], cl[1], cl[2], cl[3],
                  b->coords + 3 * cs[0], b->coords + 3 * cs[1], b->coords + 3 * cs[2], b->coords + 3 * cs[3],
                  b->nprim[cs[0]], b->exps + b->prim_off[cs[0]], b->coefs + b->prim_off[cs[0]],
                  b->nprim[cs[1]], b->exps + b->prim_off[cs[1]], b->coefs + b->prim_off[cs[1]],
@@ -1389,7 +1560,7 @@ static void cart_quartet_deriv(const orc_basis *b, const int sh[4], int which, d
     double *Gu = (double *)malloc(sizeof(double) * totu);
     const double *cfu[4] = {cf[0], cf[1], cf[2], cf[3]};
     cfu[which] = cup;
-    cart_quartet(lu[0], lu[1], lu[2], lu[3], R[0], R[1], R[2], R[3],
+    cart_quartet_any(lu[0], lu[1], lu[2], lu[3], R[0], R[1], R[2], R[3],
                  np[0], ex[0], cfu[0], np[1], ex[1], cfu[1], np[2], ex[2], cfu[2], np[3], ex[3], cfu[3],
                  kappa, Gu);
     double *Gl = NULL;
@@ -1399,7 +1570,7 @@ static void cart_quartet_deriv(const orc_basis *b, const int sh[4], int which, d
         ll[which] -= 1;
         nl[which] = NCART(ll[which]);
         Gl = (double *)malloc(sizeof(double) * (size_t)nl[0] * nl[1] * nl[2] * nl[3]);
-        cart_quartet(ll[0], ll[1], ll[2], ll[3], R[0], R[1], R[2], R[3],
+        cart_quartet_any(ll[0], ll[1], ll[2], ll[3], R[0], R[1], R[2], R[3],
                      np[0], ex[0], cf[0], np[1], ex[1], cf[1], np[2], ex[2], cf[2], np[3], ex[3], cf[3],
                      kappa, Gl);
     }

@@ -51,6 +51,11 @@ void orc_spher_norms(int nparams, int ldprim, const int *L, const int *nprim,
 
 /* ---------------- one shell quartet (auto2e frontends) ---------------- */
 int orc_eri_quartet(const orc_basis *b, int A, int B, int C, int D, double kappa, double *out);
+/* Integral scheme of all quartets: 1 (default) two-centre Hermite coefficients
+ * without the horizontal recurrence, the form the CUDA library evaluates;
+ * 0 the reference's W-matrix + HRR route (auto2e), which loses all digits on
+ * (ff|ff)-type quartets of shells that mix tight and diffuse primitives. */
+void orc_set_eri_scheme(int scheme);
 
 /* ---------------- two-step Cholesky (TwoStepCholesky*.f90) ---------------- */
 typedef struct {

@@ -74,6 +74,8 @@ def lib():
                                           C.c_int, _pl, _i64, C.c_int, C.POINTER(_Chol)]
         L.orc_stats.argtypes = [_pd, C.c_int]
         L.orc_stats_reset.argtypes = []
+        L.orc_set_eri_scheme.argtypes = [C.c_int]
+        L.orc_set_eri_scheme.restype = None
         L.orc_chol_free.argtypes = [C.POINTER(_Chol)]
         L.orc_mo_transf.argtypes = [C.POINTER(_Chol), C.POINTER(_Basis), _pi, _pd, _i64, _i64, _i64, _pd, _i64,
                                     _i64, _i64, C.c_int, _pd]
@@ -280,6 +282,14 @@ def cholesky(b: OracleBasis, tau: float, kappa: float = 0.0, want_rkpq: bool = T
 
 def stats_reset() -> None:
     lib().orc_stats_reset()
+
+
+ERI_TWO_CENTRE, ERI_REFERENCE_HRR = 1, 0
+
+
+def set_eri_scheme(scheme: int) -> None:
+    """1: two-centre Hermite form (default, as the CUDA library); 0: the reference's W-matrix + HRR."""
+    lib().orc_set_eri_scheme(int(scheme))
 
 
 def stats() -> np.ndarray:

@@ -74,18 +74,48 @@ def test_eri_permutational_symmetry_and_normalisation():
     b = O.make_basis(mol.atoms, mol.shells)
     G = O.eri_full(b)
     scale = np.max(np.abs(G))
-    # Exchanging two shells of equal l (or two pairs of equal type) reverses the
-    # direction of the horizontal recurrence or the roles of the W-matrix sides;
-    # the reference orients such quartets by their given order as well, and the
-    # recurrence's cancellation (tight f primitives a few bohr apart) makes the
-    # two orders agree only to ~1e-8 relative to the largest integral.
     for perm in [(1, 0, 2, 3), (0, 1, 3, 2), (2, 3, 0, 1)]:
-        assert np.max(np.abs(G - G.transpose(perm))) < 1e-7 * scale
+        assert np.max(np.abs(G - G.transpose(perm))) < 1e-13 * scale
     # (pq|rs) as a matrix is positive semidefinite
     n = b.nao
     M = G.reshape(n * n, n * n, order="F")
     w = np.linalg.eigvalsh(0.5 * (M + M.T))
-    assert w.min() > -1e-7 * scale
+    assert w.min() > -1e-12 * scale
+
+
+def test_two_centre_scheme_matches_reference_route():
+    """The two-centre Hermite form (what the library computes) and the
+    reference's W-matrix + HRR route give the same integrals where the HRR is
+    well conditioned: every class up to (ff|ff), 1e-10 of the largest."""
+    mol = molecules.small_molecule(5, natoms=2, recipe=(0, 1, 2, 3), nprim=(2, 3))
+    b = O.make_basis(mol.atoms, mol.shells)
+    try:
+        O.set_eri_scheme(O.ERI_REFERENCE_HRR)
+        G_ref = O.eri_full(b)
+    finally:
+        O.set_eri_scheme(O.ERI_TWO_CENTRE)
+    G = O.eri_full(b)
+    assert np.max(np.abs(G - G_ref)) < 1e-10 * np.max(np.abs(G_ref))
+
+
+def test_two_centre_scheme_stable_where_hrr_cancels():
+    """f shells mixing tight (~3e3) and diffuse (~0.07) primitives on atoms
+    4.6 bohr apart: after contraction the HRR cancels every digit of (ff|ff)
+    (bra-ket symmetry broken by a third of the largest element); the
+    two-centre form keeps the symmetry to rounding."""
+    atoms = np.array([[0.0, 0.0, 0.0], [2.9, 1.7, 3.2]])
+    sh = [(0, 3, np.array([574.8, 1.694, 0.2595, 0.1926, 0.1509, 0.06629]),
+           np.array([-0.646, 0.219, -1.279, -0.179, -0.199, -1.580])),
+          (1, 3, np.array([3321.6, 3103.6, 195.48, 0.06562]), np.array([-2.066, 0.490, 0.854, 0.162]))]
+    b = O.make_basis(atoms, sh)
+    q = O.eri_quartet(b, 0, 1, 0, 1)
+    assert np.max(np.abs(q - q.transpose(2, 3, 0, 1))) < 1e-13 * np.max(np.abs(q))
+    try:
+        O.set_eri_scheme(O.ERI_REFERENCE_HRR)
+        q_ref = O.eri_quartet(b, 0, 1, 0, 1)
+    finally:
+        O.set_eri_scheme(O.ERI_TWO_CENTRE)
+    assert np.max(np.abs(q_ref - q_ref.transpose(2, 3, 0, 1))) > 1e-3 * np.max(np.abs(q_ref))
 
 
 def test_coulomb_gradient_matches_finite_differences():
