@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--buffer-mb", type=int, default=16384)
+    ap.add_argument("--tune-pairs", type=int, default=96, help="shell pairs per class sampled by the ERI autotuner")
     ap.add_argument("--decode-storage", action="store_true",
                     help="decode diagonal-shell-pair pivots in storage order (GCI_FLAG_PIVOT_DECODE_STORAGE)")
     return ap.parse_args()
@@ -233,6 +234,12 @@ def main():
     lib_stream = torch.cuda.ExternalStream(sptr.value)
     bstruct = tb.c_struct()
     state = {"rkab": None, "nvecs": None}
+    # per-class kernel choice (team vs ket-first) by the library's autotuner, untimed set-up
+    tune = np.zeros(200)
+    t_tune = time.perf_counter()
+    _capi.check(L.gci_autotune_eri(C.byref(bstruct), args.tune_pairs, _capi.ptr(tune)))
+    t_tune = time.perf_counter() - t_tune
+    kf_classes = sum(1 for tb_ in range(10) for tk_ in range(tb_ + 1) if L.gci_eri_variant(tb_, tk_, -1) == 1)
 
     def job():
         h = C.c_void_p()
@@ -339,7 +346,8 @@ def main():
             "config": {"workload": f"{args.config}: {len(mol.atoms)} atoms, NAO={nao}, tau={mol.tau}, "
                                    f"Cholesky + AO->MO {NA}x{NB}",
                        "precision": args.precision, "nvecs": state["nvecs"], "parallelism": f"replicas x{world}",
-                       "l2": "flushed before every timed step (512 MB write outside the timed events)"},
+                       "l2": "flushed before every timed step (512 MB write outside the timed events)",
+                       "eri_autotune": {"seconds": round(t_tune, 2), "ket_first_classes": kf_classes}},
             "wall_s_per_step": t_max / args.steps, "gflop_per_step": flops_step / 1e9,
             "gflop_executed_per_step": fl["executed"] / 1e9,
             "value_definition": "reference-algorithm work (GEMM formulas + W-matrix ERI arithmetic over every "

@@ -31,32 +31,6 @@
 
 namespace gci {
 
-// ------------------------------------------------------------ compile-time index helpers
-GCI_HD constexpr int cart_level(int g) { int l = 0; while (cart_off(l + 1) <= g) ++l; return l; }
-GCI_HD constexpr int cart_x(int g) { int l = cart_level(g), p = g - cart_off(l), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return l - s; }
-GCI_HD constexpr int cart_z(int g) { int l = cart_level(g), p = g - cart_off(l), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return p - s * (s + 1) / 2; }
-GCI_HD constexpr int cart_y(int g) { return cart_level(g) - cart_x(g) - cart_z(g); }
-GCI_HD constexpr int herm_level(int h) { int n = 0; while (herm_n(n) <= h) ++n; return n; }
-GCI_HD constexpr int herm_v(int h) { int n = herm_level(h), p = h - (n > 0 ? herm_n(n - 1) : 0), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return p - s * (s + 1) / 2; }
-GCI_HD constexpr int herm_u(int h) { int n = herm_level(h), p = h - (n > 0 ? herm_n(n - 1) : 0), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return s - (p - s * (s + 1) / 2); }
-GCI_HD constexpr int herm_t(int h) { return herm_level(h) - herm_u(h) - herm_v(h); }
-GCI_HD constexpr int cmax(int a, int b) { return a > b ? a : b; }
-
-// Cartesian pair e = (a, b) of shells (la, lb), b fastest: its Hermite extent
-// along each axis and the offset of its coefficient block in a per-axis table.
-GCI_HD constexpr int pair_ga(int la, int lb, int e) { return cart_off(la) + e / ncart(lb); }
-GCI_HD constexpr int pair_gb(int la, int lb, int e) { return cart_off(lb) + e % ncart(lb); }
-GCI_HD constexpr int pair_x(int la, int lb, int e) { return cart_x(pair_ga(la, lb, e)) + cart_x(pair_gb(la, lb, e)); }
-GCI_HD constexpr int pair_y(int la, int lb, int e) { return cart_y(pair_ga(la, lb, e)) + cart_y(pair_gb(la, lb, e)); }
-GCI_HD constexpr int pair_z(int la, int lb, int e) { return cart_z(pair_ga(la, lb, e)) + cart_z(pair_gb(la, lb, e)); }
-GCI_HD constexpr int pair_ox(int la, int lb, int e) { return e2_off(la, cart_x(pair_ga(la, lb, e)), cart_x(pair_gb(la, lb, e))); }
-GCI_HD constexpr int pair_oy(int la, int lb, int e) { return e2_off(la, cart_y(pair_ga(la, lb, e)), cart_y(pair_gb(la, lb, e))); }
-GCI_HD constexpr int pair_oz(int la, int lb, int e) { return e2_off(la, cart_z(pair_ga(la, lb, e)), cart_z(pair_gb(la, lb, e))); }
-GCI_HD constexpr int pair_supp(int la, int lb, int e)
-{
-    return (pair_x(la, lb, e) + 1) * (pair_y(la, lb, e) + 1) * (pair_z(la, lb, e) + 1);
-}
-
 template <int LA, int LB, int LC, int LD>
 struct EriShape {
     static constexpr int L1 = LA + LB, L2 = LC + LD, LT = L1 + L2;
@@ -65,25 +39,19 @@ struct EriShape {
     static constexpr int HT = herm_n(LT), H1 = herm_n(L1), H2 = herm_n(L2);
     static constexpr int EA = e2_size(LA, LB), EC = e2_size(LC, LD);   // per-axis coefficient tables
     static constexpr int RSA = pp_record(LA, LB), RSB = pp_record(LC, LD);
-    static constexpr int cb_count()
-    {
-        int n = 0;
-        for (int e = 0; e < NE; ++e) n += pair_supp(LA, LB, e);
-        return n;
-    }
-    static constexpr int NCB = cb_count();
-    // team scratch (doubles): W, R ping-pong, bra products, T spill
-    static constexpr int O_W = 0, O_RA = NE * NF, O_RB = O_RA + HT, O_CB = O_RB + HT, O_TT = O_CB + NCB;
+    static constexpr int POA = pp_prod_off(LA, LB), POC = pp_prod_off(LC, LD);   // product tables
+    static constexpr int NCB = pair_ncb(LA, LB), NCK = pair_ncb(LC, LD);
+    // team scratch (doubles): W, R ping-pong, T spill
+    static constexpr int O_W = 0, O_RA = NE * NF, O_RB = O_RA + HT, O_TT = O_RB + HT;
     static constexpr int SZ_MAIN = O_TT + NE * H2;
     // epilogue ping-pong over the same scratch (P0 holds W on entry); every
     // stage has at most NE * NF elements (spherical counts <= Cartesian)
     static constexpr int SZ_P0 = NE * NF, SZ_P1 = NE * NF;
     static constexpr int SZ_TEAM = cmax(SZ_MAIN, SZ_P0 + SZ_P1);
     // per-block tables (ints)
-    static constexpr int TAB_CB = NCB;            // packed E-table offsets of each bra product
     static constexpr int TAB_RIDX = H2 * H1;      // R index of h + g
     static constexpr int TAB_HERM = HT;           // packed (t,u,v) of each Hermite index
-    static constexpr int TAB_INTS = TAB_CB + TAB_RIDX + TAB_HERM;
+    static constexpr int TAB_INTS = TAB_RIDX + TAB_HERM;
 };
 
 // Team geometry: TW lanes own the ket Hermite indices (TW >= H2).  Teams of at
@@ -123,6 +91,92 @@ __device__ __forceinline__ void set_err(int* err, int code)
     if (err) atomicCAS(err, 0, code);
 }
 
+// Epilogue of one quartet: the four one-index transforms T_D, T_C, T_B, T_A
+// (normalisation and Cartesian -> spherical) of W[ab][cd] held in P0, and the
+// scatter into the output through the row/column maps.  P1 is scratch of
+// NE * NF doubles; lanes of the team share the work.
+template <int LA, int LB, int LC, int LD, int TW, int TPB>
+__device__ __forceinline__ void eri_epilogue(const EriArgs& a, const ShellPairDev& pb, const ShellPairDev& pk,
+                                             int bra, int ket, double* P0, double* P1, int lane)
+{
+    using S = EriShape<LA, LB, LC, LD>;
+    const int A = pb.s1, B = pb.s2, C = pk.s1, D = pk.s2;
+    const int nfA = __ldg(a.sh_nfunc + A), nfB = __ldg(a.sh_nfunc + B);
+    const int nfC = __ldg(a.sh_nfunc + C), nfD = __ldg(a.sh_nfunc + D);
+    const double* __restrict__ TA = a.tmat + __ldg(a.sh_toff + A);
+    const double* __restrict__ TB = a.tmat + __ldg(a.sh_toff + B);
+    const double* __restrict__ TC = a.tmat + __ldg(a.sh_toff + C);
+    const double* __restrict__ TD = a.tmat + __ldg(a.sh_toff + D);
+    // 1) T_D on d: U[ab][c][md] (P1)
+    for (int idx = lane; idx < S::NE * S::nC * nfD; idx += TW) {
+        const int ec = idx / nfD, md = idx - ec * nfD;
+        double acc = 0.0;
+#pragma unroll
+        for (int d = 0; d < S::nD; ++d) acc += __ldg(TD + md * S::nD + d) * P0[ec * S::nD + d];
+        P1[idx] = acc;
+    }
+    team_sync<TW, TPB>();
+    // 2) T_C on c: Y[ab][mc][md] (P0)
+    const int nq = nfC * nfD;
+    for (int idx = lane; idx < S::NE * nq; idx += TW) {
+        const int e = idx / nq, q = idx - e * nq;
+        const int mc = q / nfD, md = q - mc * nfD;
+        double acc = 0.0;
+#pragma unroll
+        for (int c = 0; c < S::nC; ++c) acc += __ldg(TC + mc * S::nC + c) * P1[(e * S::nC + c) * nfD + md];
+        P0[idx] = acc;
+    }
+    team_sync<TW, TPB>();
+    // 3) T_B on b: V1[a][mb][q] (P1)
+    for (int idx = lane; idx < S::nA * nfB * nq; idx += TW) {
+        const int am = idx / nq, q = idx - am * nq;
+        const int ai = am / nfB, mb = am - ai * nfB;
+        double acc = 0.0;
+#pragma unroll
+        for (int b = 0; b < S::nB; ++b) acc += __ldg(TB + mb * S::nB + b) * P0[(ai * S::nB + b) * nq + q];
+        P1[idx] = acc;
+    }
+    team_sync<TW, TPB>();
+    // 4) T_A on a and scatter
+    const int nout = nfA * nfB * nq;
+    for (int idx = lane; idx < nout; idx += TW) {
+        const int mm = idx / nq, q = idx - mm * nq;
+        const int ma = mm / nfB, mb = mm - ma * nfB;
+        const int mc = q / nfD, md = q - mc * nfD;
+        double val = 0.0;
+#pragma unroll
+        for (int ai = 0; ai < S::nA; ++ai) val += __ldg(TA + ma * S::nA + ai) * P1[(ai * nfB + mb) * nq + q];
+        // canonical -> stored orientation of each pair
+        const int fb = pb.swap ? (mb + nfB * ma) : (ma + nfA * mb);
+        const int fk = pk.swap ? (md + nfD * mc) : (mc + nfC * md);
+        const int rowf = a.swap_bk ? fk : fb;
+        const int colf = a.swap_bk ? fb : fk;
+        if (a.mode == kModeProduct) {
+            const int row = a.row_map[a.row_off[bra] + rowf];
+            const int col = a.col_map[a.col_off[ket] + colf];
+            if (row >= 0 && col >= 0) a.out[row + a.ldo * (int64_t)col] = val;
+        } else if (a.mode == kModeDiagonal) {
+            if (rowf == colf) {
+                const int row = a.row_map[a.row_off[bra] + rowf];
+                if (row >= 0) a.out[row] = val;
+            }
+        } else {
+            // dense symmetric AO-pair layout [p][q][j]; the stored bra pair gives (p, q)
+            const ShellPairDev& ps = a.swap_bk ? pk : pb;
+            const int first = ps.swap ? ps.s2 : ps.s1;
+            const int second = ps.swap ? ps.s1 : ps.s2;
+            const int n1 = __ldg(a.sh_nfunc + first);
+            const int i1 = rowf % n1, i2 = rowf / n1;
+            const int j = a.col_map[a.col_off[ket] + colf];
+            if (j >= 0) {
+                const int64_t p = __ldg(a.sh_loc + first) + i1, qq = __ldg(a.sh_loc + second) + i2;
+                a.out[(p * a.nao + qq) * a.jcount + j] = val;
+                if (first != second) a.out[(qq * a.nao + p) * a.jcount + j] = val;
+            }
+        }
+    }
+}
+
 template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(EriTeam<LA, LB, LC, LD>::TPB)
 k_eri_class(const EriArgs a)
@@ -132,19 +186,10 @@ k_eri_class(const EriArgs a)
     constexpr int TW = G::TW, TPB = G::TPB, NT = G::NT;
     extern __shared__ double smem[];
     int* tab = reinterpret_cast<int*>(smem + (size_t)NT * G::TEAM_SZ);
-    int* tab_cb = tab;                       // (x | y << 8 | z << 16) offsets into the E tables
-    int* tab_ridx = tab + S::TAB_CB;         // [g][h] -> herm_idx(h + g)
+    int* tab_ridx = tab;                     // [g][h] -> herm_idx(h + g)
     int* tab_herm = tab_ridx + S::TAB_RIDX;  // t | u << 8 | v << 16
 
     // ---- per-block tables
-    for (int c = threadIdx.x; c < S::NCB; c += TPB) {
-        int e = 0, off = 0;
-        while (off + pair_supp(LA, LB, e) <= c) { off += pair_supp(LA, LB, e); ++e; }
-        const int ex = pair_x(LA, LB, e), ey = pair_y(LA, LB, e);
-        const int r = c - off;                       // order: v outer, u, t inner
-        const int t = r % (ex + 1), u = (r / (ex + 1)) % (ey + 1), v = r / ((ex + 1) * (ey + 1));
-        tab_cb[c] = (pair_ox(LA, LB, e) + t) | ((pair_oy(LA, LB, e) + u) << 8) | ((pair_oz(LA, LB, e) + v) << 16);
-    }
     for (int c = threadIdx.x; c < S::TAB_RIDX; c += TPB) {
         const int g = c / S::H1, h = c - g * S::H1;
         tab_ridx[c] = herm_idx(herm_t(h) + herm_t(g), herm_u(h) + herm_u(g), herm_v(h) + herm_v(g));
@@ -158,7 +203,6 @@ k_eri_class(const EriArgs a)
     double* ts = smem + (size_t)team * G::TEAM_SZ;
     double* RA = ts + S::O_RA;
     double* RB = ts + S::O_RB;
-    double* CBv = ts + S::O_CB;
     double* TT = ts + S::O_TT;
     double* WW = ts + S::O_W;
 
@@ -212,16 +256,8 @@ k_eri_class(const EriArgs a)
 #pragma unroll
                     for (int m = 0; m <= S::LT; ++m) { F[m] *= pw; pw *= m2a; }
                 }
-                // bra coefficient products Eb(e,h) = Ex Ey Ez (this bra primitive pair)
-                {
-                    const double* __restrict__ Ebx = Bp + 8;
-                    const double* __restrict__ Eby = Ebx + S::EA;
-                    const double* __restrict__ Ebz = Eby + S::EA;
-                    for (int c = lane; c < S::NCB; c += TW) {
-                        const int o = tab_cb[c];
-                        CBv[c] = __ldg(Ebx + (o & 0xff)) * __ldg(Eby + ((o >> 8) & 0xff)) * __ldg(Ebz + (o >> 16));
-                    }
-                }
+                // bra coefficient products Eb(ab, h) of this bra primitive pair
+                const double* __restrict__ CBv = Bp + S::POA;
                 // Hermite Coulomb integrals R^{(0)}_{tuv}, t+u+v <= LT
                 double* cur = RA;
                 double* nxt = RB;
@@ -267,7 +303,7 @@ k_eri_class(const EriArgs a)
                                 for (int u = 0; u <= pair_y(LA, LB, e); ++u)
 #pragma unroll
                                     for (int t = 0; t <= pair_x(LA, LB, e); ++t) {
-                                        acc += CBv[c] * Rl[herm_idx(t, u, v)];
+                                        acc += __ldg(CBv + c) * Rl[herm_idx(t, u, v)];
                                         ++c;
                                     }
                             T[e] = acc;
@@ -283,7 +319,7 @@ k_eri_class(const EriArgs a)
                                 for (int u = 0; u <= pair_y(LA, LB, e); ++u)
 #pragma unroll
                                     for (int t = 0; t <= pair_x(LA, LB, e); ++t) {
-                                        acc += CBv[c] * cur[ridx[herm_idx(t, u, v)]];
+                                        acc += __ldg(CBv + c) * cur[ridx[herm_idx(t, u, v)]];
                                         ++c;
                                     }
                             T[e] = acc;
@@ -329,83 +365,7 @@ k_eri_class(const EriArgs a)
         }
 
         // ================= epilogue: transforms + scatter =================
-        double* P0 = WW;                 // holds W[ab][cd] on entry
-        double* P1 = WW + S::SZ_P0;
-        const int A = pb.s1, B = pb.s2, C = pk.s1, D = pk.s2;
-        const int nfA = __ldg(a.sh_nfunc + A), nfB = __ldg(a.sh_nfunc + B);
-        const int nfC = __ldg(a.sh_nfunc + C), nfD = __ldg(a.sh_nfunc + D);
-        const double* __restrict__ TA = a.tmat + __ldg(a.sh_toff + A);
-        const double* __restrict__ TB = a.tmat + __ldg(a.sh_toff + B);
-        const double* __restrict__ TC = a.tmat + __ldg(a.sh_toff + C);
-        const double* __restrict__ TD = a.tmat + __ldg(a.sh_toff + D);
-        // 1) T_D on d: U[ab][c][md] (P1)
-        for (int idx = lane; idx < S::NE * S::nC * nfD; idx += TW) {
-            const int ec = idx / nfD, md = idx - ec * nfD;
-            double acc = 0.0;
-#pragma unroll
-            for (int d = 0; d < S::nD; ++d) acc += __ldg(TD + md * S::nD + d) * P0[ec * S::nD + d];
-            P1[idx] = acc;
-        }
-        team_sync<TW, TPB>();
-        // 2) T_C on c: Y[ab][mc][md] (P0)
-        const int nq = nfC * nfD;
-        for (int idx = lane; idx < S::NE * nq; idx += TW) {
-            const int e = idx / nq, q = idx - e * nq;
-            const int mc = q / nfD, md = q - mc * nfD;
-            double acc = 0.0;
-#pragma unroll
-            for (int c = 0; c < S::nC; ++c) acc += __ldg(TC + mc * S::nC + c) * P1[(e * S::nC + c) * nfD + md];
-            P0[idx] = acc;
-        }
-        team_sync<TW, TPB>();
-        // 3) T_B on b: V1[a][mb][q] (P1)
-        for (int idx = lane; idx < S::nA * nfB * nq; idx += TW) {
-            const int am = idx / nq, q = idx - am * nq;
-            const int ai = am / nfB, mb = am - ai * nfB;
-            double acc = 0.0;
-#pragma unroll
-            for (int b = 0; b < S::nB; ++b) acc += __ldg(TB + mb * S::nB + b) * P0[(ai * S::nB + b) * nq + q];
-            P1[idx] = acc;
-        }
-        team_sync<TW, TPB>();
-        // 4) T_A on a and scatter
-        const int nout = nfA * nfB * nq;
-        for (int idx = lane; idx < nout; idx += TW) {
-            const int mm = idx / nq, q = idx - mm * nq;
-            const int ma = mm / nfB, mb = mm - ma * nfB;
-            const int mc = q / nfD, md = q - mc * nfD;
-            double val = 0.0;
-#pragma unroll
-            for (int ai = 0; ai < S::nA; ++ai) val += __ldg(TA + ma * S::nA + ai) * P1[(ai * nfB + mb) * nq + q];
-            // canonical -> stored orientation of each pair
-            const int fb = pb.swap ? (mb + nfB * ma) : (ma + nfA * mb);
-            const int fk = pk.swap ? (md + nfD * mc) : (mc + nfC * md);
-            const int rowf = a.swap_bk ? fk : fb;
-            const int colf = a.swap_bk ? fb : fk;
-            if (a.mode == kModeProduct) {
-                const int row = a.row_map[a.row_off[bra] + rowf];
-                const int col = a.col_map[a.col_off[ket] + colf];
-                if (row >= 0 && col >= 0) a.out[row + a.ldo * (int64_t)col] = val;
-            } else if (a.mode == kModeDiagonal) {
-                if (rowf == colf) {
-                    const int row = a.row_map[a.row_off[bra] + rowf];
-                    if (row >= 0) a.out[row] = val;
-                }
-            } else {
-                // dense symmetric AO-pair layout [p][q][j]; the stored bra pair gives (p, q)
-                const ShellPairDev& ps = a.swap_bk ? pk : pb;
-                const int first = ps.swap ? ps.s2 : ps.s1;
-                const int second = ps.swap ? ps.s1 : ps.s2;
-                const int n1 = __ldg(a.sh_nfunc + first);
-                const int i1 = rowf % n1, i2 = rowf / n1;
-                const int j = a.col_map[a.col_off[ket] + colf];
-                if (j >= 0) {
-                    const int64_t p = __ldg(a.sh_loc + first) + i1, qq = __ldg(a.sh_loc + second) + i2;
-                    a.out[(p * a.nao + qq) * a.jcount + j] = val;
-                    if (first != second) a.out[(qq * a.nao + p) * a.jcount + j] = val;
-                }
-            }
-        }
+        eri_epilogue<LA, LB, LC, LD, TW, TPB>(a, pb, pk, bra, ket, WW, WW + S::SZ_P0, lane);
         team_sync<TW, TPB>();
     }
 }

@@ -72,6 +72,21 @@ __global__ void k_pair_records(const ShellPairDev* __restrict__ pairs, int npair
                         }
                     }
             }
+            // Hermite products of every Cartesian pair (b fastest), v outer, t inner
+            const double* Ex = rec + 8;
+            const double* Ey = Ex + ne;
+            const double* Ez = Ey + ne;
+            double* prod = rec + pp_prod_off(la, lb);
+            int c = 0;
+            for (int e = 0; e < ncart(la) * ncart(lb); ++e) {
+                const int ex = pair_x(la, lb, e), ey = pair_y(la, lb, e), ez = pair_z(la, lb, e);
+                const int ox = pair_ox(la, lb, e), oy = pair_oy(la, lb, e), oz = pair_oz(la, lb, e);
+                for (int v = 0; v <= ez; ++v)
+                    for (int u = 0; u <= ey; ++u) {
+                        const double yz = Ey[oy + u] * Ez[oz + v];
+                        for (int t = 0; t <= ex; ++t) prod[c++] = Ex[ox + t] * yz;
+                    }
+            }
         }
     }
 }
@@ -86,7 +101,9 @@ __global__ void k_boys_eval(int m, int64_t n, const double* __restrict__ x, cons
     }
 }
 
-static LaunchFn g_launch[kNumPairTypes][kNumPairTypes];
+static LaunchFn g_launch[kNumPairTypes][kNumPairTypes];      // team kernels, every canonical class
+static LaunchFn g_launch_kf[kNumPairTypes][kNumPairTypes];   // ket-first kernels where built
+static int g_variant[kNumPairTypes][kNumPairTypes];          // 0 team, 1 ket-first
 
 cudaError_t eri_module_init()
 {
@@ -96,20 +113,36 @@ cudaError_t eri_module_init()
     register_eri_classes_b(g_launch);
     register_eri_classes_c(g_launch);
     register_eri_classes_d(g_launch);
+    register_eri_kf_a(g_launch_kf);
+    register_eri_kf_b(g_launch_kf);
+    register_eri_kf_c(g_launch_kf);
+    register_eri_kf_d(g_launch_kf);
+    for (int tb = 0; tb < kNumPairTypes; ++tb)
+        for (int tk = 0; tk <= tb; ++tk) g_variant[tb][tk] = g_launch_kf[tb][tk] ? 1 : 0;
     done = true;
     return cudaSuccess;
 }
 
-int eri_team_width(int tb, int tk)
+int eri_variant(int tb, int tk)
 {
-    (void)tb; (void)tk;
+    if (tb < 0 || tk < 0 || tb >= kNumPairTypes || tk >= kNumPairTypes || tb < tk) return -1;
+    return g_variant[tb][tk];
+}
+
+int eri_set_variant(int tb, int tk, int variant)
+{
+    if (tb < 0 || tk < 0 || tb >= kNumPairTypes || tk >= kNumPairTypes || tb < tk) return -1;
+    if (variant == 1 && !g_launch_kf[tb][tk]) return -1;
+    if (variant != 0 && variant != 1) return -1;
+    g_variant[tb][tk] = variant;
     return 0;
 }
 
 cudaError_t eri_launch(int tb, int tk, const EriArgs& args, cudaStream_t st)
 {
     if (tb < 0 || tk < 0 || tb >= kNumPairTypes || tk >= kNumPairTypes || tb < tk) return cudaErrorInvalidValue;
-    g_launch[tb][tk](args, st);
+    LaunchFn fn = (g_variant[tb][tk] == 1) ? g_launch_kf[tb][tk] : g_launch[tb][tk];
+    fn(args, st);
     count_launch();
     return cudaGetLastError();
 }

@@ -1,0 +1,10 @@
+// eri_kf_b.cu -- ket-first ERI class kernels with bra pair types [6, 7].
+#include "eri_classes.cuh"
+
+namespace gci {
+void register_eri_kf_b(LaunchFn (*tab)[kNumPairTypes])
+{
+    register_row_kf<6>(tab);
+    register_row_kf<7>(tab);
+}
+} // namespace gci

@@ -1470,6 +1470,87 @@ int gci_eri_pairs(const gci_basis* basis, double omega, double* out, int64_t ld)
     });
 }
 
+int gci_eri_variant(int tb, int tk, int variant)
+{
+    const int rc = guarded([&] {
+        CU(eri_module_init());
+        if (variant >= 0 && eri_set_variant(tb, tk, variant) != 0)
+            fail(GCI_ERR_ARG, "ERI kernel variant " + std::to_string(variant) + " is not available for class (" +
+                                  std::to_string(tb) + "|" + std::to_string(tk) + ")");
+        if (eri_variant(tb, tk) < 0) fail(GCI_ERR_ARG, "invalid ERI class");
+    });
+    return rc == GCI_OK ? eri_variant(tb, tk) : rc;
+}
+
+int gci_autotune_eri(const gci_basis* basis, int max_pairs, double* seconds)
+{
+    if (max_pairs <= 0) { g_last_error = "max_pairs must be positive"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        Context& C = ctx();
+        Handle H;
+        H.timer.s = C.stream;
+        H.hb = make_basis(basis);
+        setup_pairs(H);
+        const PairTable& P = H.pt;
+        std::vector<std::vector<int>> by_type(kNumPairTypes);
+        for (int64_t sp = 0; sp < P.n; ++sp)
+            if ((int)by_type[P.type[sp]].size() < max_pairs) by_type[P.type[sp]].push_back((int)sp);
+        // every slot of the sampled pairs maps into a 1024 x 1024 scratch (collisions are
+        // harmless: only the launch time is measured)
+        constexpr int kSide = 1024;
+        PairMap m;
+        m.reset(P.n);
+        for (int t = 0; t < kNumPairTypes; ++t)
+            for (int id : by_type[t]) {
+                int* mm = m.add(id, P.nab[id]);
+                for (int i = 0; i < P.nab[id]; ++i) mm[i] = (id * 37 + i) % kSide;
+            }
+        m.upload(C.stream);
+        DVec<double> out;
+        out.alloc((size_t)kSide * kSide);
+        cudaEvent_t e0, e1;
+        CU(cudaEventCreate(&e0));
+        CU(cudaEventCreate(&e1));
+        std::vector<double> times((size_t)kNumPairTypes * kNumPairTypes * 2, 0.0);
+        try {
+            for (int tb = 0; tb < kNumPairTypes; ++tb)
+                for (int tk = 0; tk <= tb; ++tk) {
+                    if (by_type[tb].empty() || by_type[tk].empty()) continue;
+                    const int keep = eri_variant(tb, tk);
+                    if (eri_set_variant(tb, tk, 1) != 0) continue;   // one kernel only: nothing to choose
+                    eri_set_variant(tb, tk, keep);
+                    double best[2] = {-1.0, -1.0};
+                    for (int v = 0; v < 2; ++v) {
+                        if (eri_set_variant(tb, tk, v) != 0) continue;
+                        run_eri(H, by_type[tb], by_type[tk], kModeProduct, &m, &m, out.p, kSide);   // warm-up
+                        float ms = 0.0f, msmin = 1e30f;
+                        for (int rep = 0; rep < 2; ++rep) {
+                            CU(cudaEventRecord(e0, C.stream));
+                            run_eri(H, by_type[tb], by_type[tk], kModeProduct, &m, &m, out.p, kSide);
+                            CU(cudaEventRecord(e1, C.stream));
+                            CU(cudaEventSynchronize(e1));
+                            CU(cudaEventElapsedTime(&ms, e0, e1));
+                            msmin = std::min(msmin, ms);
+                        }
+                        best[v] = 1e-3 * msmin;
+                        times[((size_t)tb * kNumPairTypes + tk) * 2 + v] = best[v];
+                    }
+                    int pick = keep;
+                    if (best[0] >= 0.0 && best[1] >= 0.0) pick = best[1] < best[0] ? 1 : 0;
+                    else if (best[0] >= 0.0) pick = 0;
+                    eri_set_variant(tb, tk, pick);
+                }
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (seconds) std::copy(times.begin(), times.end(), seconds);
+    });
+}
+
 int gci_eri_pairs_noalloc(const gci_basis* basis, double omega, double* out_dev, int64_t ld, void* stream)
 {
     if (!out_dev) { g_last_error = "out_dev is NULL"; return GCI_ERR_ARG; }

@@ -45,9 +45,48 @@ GCI_HD constexpr int e2_off(int la, int i, int j)
 }
 GCI_HD constexpr int e2_size(int la, int lb) { return (la + 1) * (lb + 1) * (la + lb + 2) / 2; }
 
-// Size in doubles of one primitive-pair record of a pair (l1, l2):
-//   [0] P  [1..3] Rp  [4] K_ab c_a c_b  [5..7] Rp - A  [8..] E^{ij}_t, x/y/z tables
-GCI_HD constexpr int pp_record(int l1, int l2) { return 8 + 3 * e2_size(l1, l2); }
+// ------------------------------------------------------------ index helpers (compile time and device)
+GCI_HD constexpr int cart_level(int g) { int l = 0; while (cart_off(l + 1) <= g) ++l; return l; }
+GCI_HD constexpr int cart_x(int g) { int l = cart_level(g), p = g - cart_off(l), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return l - s; }
+GCI_HD constexpr int cart_z(int g) { int l = cart_level(g), p = g - cart_off(l), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return p - s * (s + 1) / 2; }
+GCI_HD constexpr int cart_y(int g) { return cart_level(g) - cart_x(g) - cart_z(g); }
+GCI_HD constexpr int herm_level(int h) { int n = 0; while (herm_n(n) <= h) ++n; return n; }
+GCI_HD constexpr int herm_v(int h) { int n = herm_level(h), p = h - (n > 0 ? herm_n(n - 1) : 0), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return p - s * (s + 1) / 2; }
+GCI_HD constexpr int herm_u(int h) { int n = herm_level(h), p = h - (n > 0 ? herm_n(n - 1) : 0), s = 0; while ((s + 1) * (s + 2) / 2 <= p) ++s; return s - (p - s * (s + 1) / 2); }
+GCI_HD constexpr int herm_t(int h) { return herm_level(h) - herm_u(h) - herm_v(h); }
+GCI_HD constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+// Cartesian pair e = (a, b) of shells (la, lb), b fastest: its Hermite extent
+// along each axis and the offset of its coefficient block in a per-axis table.
+GCI_HD constexpr int pair_ga(int la, int lb, int e) { return cart_off(la) + e / ncart(lb); }
+GCI_HD constexpr int pair_gb(int la, int lb, int e) { return cart_off(lb) + e % ncart(lb); }
+GCI_HD constexpr int pair_x(int la, int lb, int e) { return cart_x(pair_ga(la, lb, e)) + cart_x(pair_gb(la, lb, e)); }
+GCI_HD constexpr int pair_y(int la, int lb, int e) { return cart_y(pair_ga(la, lb, e)) + cart_y(pair_gb(la, lb, e)); }
+GCI_HD constexpr int pair_z(int la, int lb, int e) { return cart_z(pair_ga(la, lb, e)) + cart_z(pair_gb(la, lb, e)); }
+GCI_HD constexpr int pair_ox(int la, int lb, int e) { return e2_off(la, cart_x(pair_ga(la, lb, e)), cart_x(pair_gb(la, lb, e))); }
+GCI_HD constexpr int pair_oy(int la, int lb, int e) { return e2_off(la, cart_y(pair_ga(la, lb, e)), cart_y(pair_gb(la, lb, e))); }
+GCI_HD constexpr int pair_oz(int la, int lb, int e) { return e2_off(la, cart_z(pair_ga(la, lb, e)), cart_z(pair_gb(la, lb, e))); }
+GCI_HD constexpr int pair_supp(int la, int lb, int e)
+{
+    return (pair_x(la, lb, e) + 1) * (pair_y(la, lb, e) + 1) * (pair_z(la, lb, e) + 1);
+}
+
+// Number of Hermite products E^{ab}_{tuv} = E^x E^y E^z over all Cartesian pairs
+// of shells (la, lb): the product table of a primitive-pair record.
+GCI_HD constexpr int pair_ncb(int la, int lb)
+{
+    int n = 0;
+    for (int e = 0; e < ncart(la) * ncart(lb); ++e) n += pair_supp(la, lb, e);
+    return n;
+}
+
+// Primitive-pair record of a pair (l1, l2), in doubles:
+//   [0] P  [1..3] Rp  [4] K_ab c_a c_b  [5..7] Rp - A
+//   [8 ..]            E^{ij}_t tables for x, y, z (e2_size each)
+//   [8 + 3 e2_size ..] products E^{ab}_{tuv} for every Cartesian pair ab
+//                      (b fastest), each over v outer, u, t inner
+GCI_HD constexpr int pp_prod_off(int l1, int l2) { return 8 + 3 * e2_size(l1, l2); }
+GCI_HD constexpr int pp_record(int l1, int l2) { return pp_prod_off(l1, l2) + pair_ncb(l1, l2); }
 
 // Output modes of the ERI kernels.
 enum EriMode : int {

@@ -158,6 +158,23 @@ int gci_normalize_basis(int64_t nparams, int64_t ldprim, const int64_t *L, const
  * triangle for ShA == ShB).  Small bases only (tests). */
 int gci_eri_pairs(const gci_basis *basis, double omega, double *out, int64_t ld);
 
+/* ---- ERI kernel selection (no counterpart in the reference) ---- */
+
+/* Each ERI class (pair types tb >= tk, pair type = lhi*(lhi+1)/2 + llo of the
+ * two shells' angular momenta) has a team kernel (variant 0: lanes over the
+ * ket Hermite indices, every class) and, for bra types from (d,s) up and ket
+ * types up to (f,p), a ket-first warp kernel (variant 1).
+ * gci_eri_variant(tb, tk, v): v = 0 or 1 selects, v < 0 only queries; returns
+ * the variant in use (>= 0) or GCI_ERR_ARG.  The choice is process-wide. */
+int gci_eri_variant(int tb, int tk, int variant);
+
+/* Autotuner: times both variants of every class that occurs in `basis` on a
+ * product-mode sample of its shell pairs (up to max_pairs bra and max_pairs
+ * ket pairs per class) with CUDA events and keeps the faster one.  If
+ * `seconds` is not NULL it receives 10 x 10 x 2 launch times (tb, tk,
+ * variant; 0 where not measured). */
+int gci_autotune_eri(const gci_basis *basis, int max_pairs, double *seconds);
+
 /* ---- allocation-free entry point (no counterpart in the reference) ---- */
 
 /* Size of the fixed device scratch behind gci_eri_pairs_noalloc: a file-scope

@@ -1,7 +1,7 @@
 """GPU parity tests: libgci.so (through the C ABI) against the CPU oracle.
 
-Tolerances: Boys 1e-13 relative (same table scheme); ERIs 1e-10 relative to
-the largest integral (FP64 rounding of the HRR differs between orientations);
+Tolerances: Boys 1e-13 relative (same table scheme); ERIs 1e-12 relative to
+the largest integral (same two-centre Hermite form, different summation order);
 reconstructed (pq|rs) = sum_k R_kpq R_krs and MO integrals within 1e-8
 absolute of the oracle's own reconstructions; identical pivot sequences.
 """
@@ -51,16 +51,52 @@ def _vdiag_order_pairs(ob):
     return np.array(pairs)
 
 
+class _Variants:
+    """Force one ERI kernel variant on every class that has it; restore on exit."""
+
+    def __init__(self, lib, variant):
+        self.lib, self.variant, self.saved = lib, variant, {}
+
+    def __enter__(self):
+        for tb in range(10):
+            for tk in range(tb + 1):
+                self.saved[(tb, tk)] = self.lib.gci_eri_variant(tb, tk, -1)
+                self.lib.gci_eri_variant(tb, tk, self.variant)   # GCI_ERR_ARG where not built
+        return self
+
+    def __exit__(self, *exc):
+        for (tb, tk), v in self.saved.items():
+            self.lib.gci_eri_variant(tb, tk, v)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("recipe,seed,natoms", [(molecules.RECIPE_C1, 11, 3), (molecules.RECIPE_C2, 12, 2)])
-def test_eri_blocks_all_classes(gpu_lib, recipe, seed, natoms):
+def test_eri_blocks_all_classes(gpu_lib, recipe, seed, natoms, variant):
     mol = molecules.small_molecule(seed, natoms=natoms, recipe=recipe, nprim=(3, 4))
     tb, ob = both(mol)
-    V = _eri_pairs_gpu(tb)
+    with _Variants(gpu_lib, variant):
+        V = _eri_pairs_gpu(tb)
     G = O.eri_full(ob)
     pq = _vdiag_order_pairs(ob)
     ref = G[pq[:, 0], pq[:, 1]][:, pq[:, 0], pq[:, 1]]
     err = np.max(np.abs(V - ref))
-    assert err < 1e-10 * max(1.0, np.max(np.abs(ref))), err
+    # two-centre Hermite form in both: agreement to rounding of the largest integral
+    assert err < 1e-12 * max(1.0, np.max(np.abs(ref))), err
+
+
+def test_autotune_keeps_results(gpu_lib):
+    mol = molecules.small_molecule(12, natoms=2, recipe=molecules.RECIPE_C2, nprim=(3, 4))
+    tb, ob = both(mol)
+    secs = np.zeros(200)
+    s = tb.c_struct()
+    import ctypes as C
+    _capi.check(gpu_lib.gci_autotune_eri(C.byref(s), 64, _capi.ptr(secs)))
+    assert np.all(secs >= 0) and np.count_nonzero(secs) > 0
+    V = _eri_pairs_gpu(tb)
+    G = O.eri_full(ob)
+    pq = _vdiag_order_pairs(ob)
+    ref = G[pq[:, 0], pq[:, 1]][:, pq[:, 0], pq[:, 1]]
+    assert np.max(np.abs(V - ref)) < 1e-12 * max(1.0, np.max(np.abs(ref)))
 
 
 def _shellpair_of_full(ch):
