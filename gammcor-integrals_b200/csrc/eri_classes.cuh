@@ -33,9 +33,9 @@ static void launch_class(const EriArgs& args, cudaStream_t st)
     kern<<<(unsigned)blocks, G::TPB, smem, st>>>(args);
 }
 
-// Ket-first warp kernel (eri_ketfirst.cuh), built for bra types from (d,s)
-// up and ket types up to (f,p): one warp per quartet, grid capped at 64
-// blocks per SM with a grid-stride loop inside.
+// Ket-first kernel (eri_ketfirst.cuh), built for bra types from (d,s) up:
+// a warp or a 128-thread block per quartet, grid capped at 64 blocks per SM
+// with a grid-stride loop inside.
 template <int TB, int TK>
 static void launch_kf(const EriArgs& args, cudaStream_t st)
 {
@@ -56,7 +56,7 @@ static void launch_kf(const EriArgs& args, cudaStream_t st)
     kern<<<(unsigned)blocks, K::TPB, smem, st>>>(args);
 }
 
-constexpr bool has_kf(int tb, int tk) { return tb >= 3 && tk <= 7; }
+constexpr bool has_kf(int tb, int tk) { return tb >= 3 && tk <= tb; }
 
 template <int TB, int TK = TB>
 static void register_row_kf(LaunchFn (*tab)[kNumPairTypes])

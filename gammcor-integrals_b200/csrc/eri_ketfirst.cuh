@@ -49,20 +49,27 @@ struct KfShape {
     static constexpr int SLOTS = (S::H1 + TW - 1) / TW;        // bra Hermite indices per lane
     static constexpr int WSLOTS = (S::NE * S::NF + TW - 1) / TW;
     static constexpr bool WREG = WSLOTS <= 40;                 // W in registers, else shared memory
-    // ket pairs per chunk of the primitive loop: V (SLOTS x CH) and the lane's
-    // R values (H2) within ~88 doubles
-    static constexpr int CH0 = (88 - S::H2) / SLOTS;
+    // R(h + g) of a lane's bra Hermite indices held in registers (RL) or read
+    // from shared memory per product (large ket classes)
+    static constexpr bool RL = S::H2 <= 56;
+    // ket pairs per chunk of the primitive loop: V (SLOTS x CH) and, with RL,
+    // the lane's R values (H2) within ~88 doubles
+    static constexpr int CH0 = RL ? (88 - S::H2) / SLOTS : 80 / SLOTS;
     static constexpr int CH = CH0 < 1 ? 1 : (CH0 > S::NF ? S::NF : CH0);
     static constexpr int NCH = (S::NF + CH - 1) / CH;
-    // team scratch (doubles): R ping-pong and V during the primitive loop; the
-    // epilogue's two buffers of NE*NF afterwards (W in registers) or W kept
-    // apart from them (W in shared memory)
-    static constexpr int O_RA = 0, O_RB = S::HT, O_V = 2 * S::HT;
-    static constexpr int SZ_LOOP = O_V + S::H1 * S::NF;
+    // ket primitive pairs whose Boys values and geometry are prepared at once
+    // (one per lane) and the stride of their entries: F_0..F_LT, X, Y, Z
+    static constexpr int KB = 32, FS = S::LT + 4;
+    // team scratch (doubles): R ping-pong, V and the prepared ket primitives
+    // during the primitive loop; the epilogue's two buffers of NE*NF
+    // afterwards (W in registers) or W kept apart from them (W in shared memory)
+    static constexpr int O_RA = 0, O_RB = S::HT, O_V = 2 * S::HT, O_FK = O_V + S::H1 * S::NF;
+    static constexpr int SZ_LOOP = O_FK + KB * FS;
     static constexpr int O_W = WREG ? 0 : cmax(SZ_LOOP, S::NE * S::NF);
     static constexpr int SZ = WREG ? cmax(SZ_LOOP, 2 * S::NE * S::NF) : O_W + S::NE * S::NF;
-    // per-block tables (ints): packed Hermite (t,u,v); R index of h + g;
-    // Hermite index of every bra product; first bra product of each ab
+    // per-block tables: R recursion recipe of every Hermite index (its
+    // coefficient as a double, then ints: source indices and axis); R index
+    // of h + g; Hermite index of every bra product; first bra product of each ab
     static constexpr int TAB_INTS = S::HT + S::H2 * S::H1 + S::NCB + S::NE + 1;
     // teams per block: four warps while their scratch stays within 160 KB
     static constexpr int TEAMS = TW == 128 ? 1
@@ -71,7 +78,7 @@ struct KfShape {
     static constexpr int TPB = TW == 128 ? 128 : 32 * TEAMS;
     static constexpr size_t smem_bytes()
     {
-        return sizeof(double) * (size_t)TEAMS * SZ + sizeof(int) * (size_t)TAB_INTS;
+        return sizeof(double) * ((size_t)TEAMS * SZ + S::HT) + sizeof(int) * (size_t)TAB_INTS;
     }
 };
 
@@ -83,12 +90,23 @@ k_eri_kf(const EriArgs a)
     using K = KfShape<LA, LB, LC, LD>;
     constexpr int TW = K::TW, TPB = K::TPB;
     extern __shared__ double smem[];
-    int* tab_herm = reinterpret_cast<int*>(smem + (size_t)K::TEAMS * K::SZ);
-    int* tab_ridx = tab_herm + S::HT;            // [g][h] -> herm_idx(h + g)
+    double* tab_coef = smem + (size_t)K::TEAMS * K::SZ;           // recursion coefficient of h
+    int* tab_rec = reinterpret_cast<int*>(tab_coef + S::HT);       // i1 | i2 << 12 | axis << 24
+    int* tab_ridx = tab_rec + S::HT;             // [g][h] -> herm_idx(h + g)
     int* tab_cbh = tab_ridx + S::H2 * S::H1;     // bra product -> Hermite index
     int* tab_cbo = tab_cbh + S::NCB;             // ab -> first bra product
 
-    for (int c = threadIdx.x; c < S::HT; c += TPB) tab_herm[c] = herm_t(c) | (herm_u(c) << 8) | (herm_v(c) << 16);
+    // R^{(j)}_{tuv} = d R^{(j+1)}_{tuv - e} + (n - 1) R^{(j+1)}_{tuv - 2e} along the first
+    // nonzero axis e of (t,u,v) with component n (d = X, Y or Z); h = 0 takes F_j
+    for (int c = threadIdx.x; c < S::HT; c += TPB) {
+        const int t = herm_t(c), u = herm_u(c), v = herm_v(c);
+        int ax = 3, i1 = 0, i2 = 0, n = 0;
+        if (t > 0) { ax = 0; n = t; i1 = herm_idx(t - 1, u, v); i2 = t > 1 ? herm_idx(t - 2, u, v) : 0; }
+        else if (u > 0) { ax = 1; n = u; i1 = herm_idx(t, u - 1, v); i2 = u > 1 ? herm_idx(t, u - 2, v) : 0; }
+        else if (v > 0) { ax = 2; n = v; i1 = herm_idx(t, u, v - 1); i2 = v > 1 ? herm_idx(t, u, v - 2) : 0; }
+        tab_rec[c] = i1 | (i2 << 12) | (ax << 24);
+        tab_coef[c] = n > 1 ? (double)(n - 1) : 0.0;
+    }
     for (int c = threadIdx.x; c < S::H2 * S::H1; c += TPB) {
         const int g = c / S::H1, h = c - g * S::H1;
         tab_ridx[c] = herm_idx(herm_t(h) + herm_t(g), herm_u(h) + herm_u(g), herm_v(h) + herm_v(g));
@@ -112,6 +130,7 @@ k_eri_kf(const EriArgs a)
     double* RB = ts + K::O_RB;
     double* V = ts + K::O_V;
     double* Ws = ts + K::O_W;
+    double* Fk = ts + K::O_FK;
 
     const int64_t ntasks = (a.mode == kModeDiagonal) ? a.nbra : a.nbra * a.nket;
     const int64_t stride = (int64_t)gridDim.x * K::TEAMS;
@@ -156,81 +175,87 @@ k_eri_kf(const EriArgs a)
 #pragma unroll
                     for (int f = 0; f < K::CH; ++f) Vr[s][f] = 0.0;
 
-                for (int kp = 0; kp < nkp; ++kp) {
-                    const double* __restrict__ Kp = rk + (size_t)kp * S::RSB;
-                    const double Q = __ldg(Kp + 0);
-                    const double X = px - __ldg(Kp + 1), Y = py - __ldg(Kp + 2), Z = pz - __ldg(Kp + 3);
-                    const double PQ = P * Q;
-                    const double den = P + Q + a.kappa * PQ;
-                    const double alpha = PQ / den;
-                    // 2 pi^{5/2} / (PQ sqrt(P+Q+kappa PQ)) (auto2e_WMatrix_part1.f90:134)
-                    const double pref = 34.986836655249725 / (PQ * sqrt(den)) * pab * __ldg(Kp + 4);
-                    double F[S::LT + 1];
-                    boys_fm<S::LT>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
-                    {
+                for (int k0 = 0; k0 < nkp; k0 += K::KB) {
+                    const int kn = (nkp - k0) < K::KB ? (nkp - k0) : K::KB;
+                    // Boys values (scaled by the prefactor and (-2 alpha)^m) and P - Q of
+                    // this bra primitive with up to KB ket primitives, one per lane
+                    for (int kk = lane; kk < kn; kk += TW) {
+                        const double* __restrict__ Kp = rk + (size_t)(k0 + kk) * S::RSB;
+                        const double Q = __ldg(Kp + 0);
+                        const double X = px - __ldg(Kp + 1), Y = py - __ldg(Kp + 2), Z = pz - __ldg(Kp + 3);
+                        const double PQ = P * Q;
+                        const double den = P + Q + a.kappa * PQ;
+                        const double alpha = PQ / den;
+                        // 2 pi^{5/2} / (PQ sqrt(P+Q+kappa PQ)) (auto2e_WMatrix_part1.f90:134)
+                        const double pref = 34.986836655249725 / (PQ * sqrt(den)) * pab * __ldg(Kp + 4);
+                        double F[S::LT + 1];
+                        boys_fm<S::LT>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
+                        double* fk = Fk + kk * K::FS;
                         double pw = pref;
                         const double m2a = -2.0 * alpha;
 #pragma unroll
-                        for (int m = 0; m <= S::LT; ++m) { F[m] *= pw; pw *= m2a; }
+                        for (int m = 0; m <= S::LT; ++m) { fk[m] = F[m] * pw; pw *= m2a; }
+                        fk[S::LT + 1] = X; fk[S::LT + 2] = Y; fk[S::LT + 3] = Z;
                     }
-                    // Hermite Coulomb integrals R^{(0)}_{tuv}, t+u+v <= LT (Helgaker 9.9.18-20)
-                    double* cur = RA;
-                    double* nxt = RB;
-                    if (lane == 0) cur[0] = F[S::LT];
                     team_sync<TW, TPB>();
+                    for (int kk = 0; kk < kn; ++kk) {
+                        const double* __restrict__ Kp = rk + (size_t)(k0 + kk) * S::RSB;
+                        const double* fk = Fk + kk * K::FS;
+                        const double X = fk[S::LT + 1], Y = fk[S::LT + 2], Z = fk[S::LT + 3];
+                        // Hermite Coulomb integrals R^{(0)}_{tuv}, t+u+v <= LT (Helgaker 9.9.18-20)
+                        double* cur = RA;
+                        double* nxt = RB;
+                        if (lane == 0) cur[0] = fk[S::LT];
+                        team_sync<TW, TPB>();
 #pragma unroll
-                    for (int j = S::LT - 1; j >= 0; --j) {
-                        const int nent = herm_n(S::LT - j);
-                        for (int h = lane; h < nent; h += TW) {
-                            const int p = tab_herm[h];
-                            const int t = p & 0xff, u = (p >> 8) & 0xff, v = p >> 16;
-                            double r;
-                            if (t > 0) {
-                                r = X * cur[herm_idx(t - 1, u, v)];
-                                if (t > 1) r += (double)(t - 1) * cur[herm_idx(t - 2, u, v)];
-                            } else if (u > 0) {
-                                r = Y * cur[herm_idx(t, u - 1, v)];
-                                if (u > 1) r += (double)(u - 1) * cur[herm_idx(t, u - 2, v)];
-                            } else if (v > 0) {
-                                r = Z * cur[herm_idx(t, u, v - 1)];
-                                if (v > 1) r += (double)(v - 1) * cur[herm_idx(t, u, v - 2)];
-                            } else {
-                                r = F[j];
+                        for (int j = S::LT - 1; j >= 0; --j) {
+                            const int nent = herm_n(S::LT - j);
+                            const double Fj = fk[j];
+                            for (int h = lane; h < nent; h += TW) {
+                                const int rc = tab_rec[h];
+                                const int ax = rc >> 24;
+                                const double d = ax == 0 ? X : (ax == 1 ? Y : Z);
+                                const double r = d * cur[rc & 0xfff] + tab_coef[h] * cur[(rc >> 12) & 0xfff];
+                                nxt[h] = (h == 0) ? Fj : r;
                             }
-                            nxt[h] = r;
+                            team_sync<TW, TPB>();
+                            double* tmp = cur; cur = nxt; nxt = tmp;
+                        }
+                        // V(h, cd) += sum_g (-1)^|g| Ek(cd, g) R(h + g), lane owns h = lane + TW s
+                        const double* __restrict__ Ck = Kp + S::POC + c0;
+#pragma unroll
+                        for (int s = 0; s < K::SLOTS; ++s) {
+                            const int h = lane + TW * s;
+                            if (h < S::H1) {
+                                double Rl[K::RL ? S::H2 : 1];
+                                if constexpr (K::RL) {
+#pragma unroll
+                                    for (int g = 0; g < S::H2; ++g) Rl[g] = cur[tab_ridx[g * S::H1 + h]];
+                                }
+                                int c = 0;
+#pragma unroll
+                                for (int f = f0; f < f1; ++f) {
+                                    double acc = Vr[s][f - f0];
+#pragma unroll
+                                    for (int v = 0; v <= pair_z(LC, LD, f); ++v)
+#pragma unroll
+                                        for (int u = 0; u <= pair_y(LC, LD, f); ++u)
+#pragma unroll
+                                            for (int t = 0; t <= pair_x(LC, LD, f); ++t) {
+                                                const double e = __ldg(Ck + c);
+                                                double rv;
+                                                if constexpr (K::RL) rv = Rl[herm_idx(t, u, v)];
+                                                else rv = cur[tab_ridx[herm_idx(t, u, v) * S::H1 + h]];
+                                                if ((t + u + v) & 1) acc -= e * rv;
+                                                else acc += e * rv;
+                                                ++c;
+                                            }
+                                    Vr[s][f - f0] = acc;
+                                }
+                            }
                         }
                         team_sync<TW, TPB>();
-                        double* tmp = cur; cur = nxt; nxt = tmp;
                     }
-                    // V(h, cd) += sum_g (-1)^|g| Ek(cd, g) R(h + g), lane owns h = lane + TW s
-                    const double* __restrict__ Ck = Kp + S::POC + c0;
-#pragma unroll
-                    for (int s = 0; s < K::SLOTS; ++s) {
-                        const int h = lane + TW * s;
-                        if (h < S::H1) {
-                            double Rl[S::H2];
-#pragma unroll
-                            for (int g = 0; g < S::H2; ++g) Rl[g] = cur[tab_ridx[g * S::H1 + h]];
-                            int c = 0;
-#pragma unroll
-                            for (int f = f0; f < f1; ++f) {
-                                double acc = Vr[s][f - f0];
-#pragma unroll
-                                for (int v = 0; v <= pair_z(LC, LD, f); ++v)
-#pragma unroll
-                                    for (int u = 0; u <= pair_y(LC, LD, f); ++u)
-#pragma unroll
-                                        for (int t = 0; t <= pair_x(LC, LD, f); ++t) {
-                                            const double e = __ldg(Ck + c);
-                                            if ((t + u + v) & 1) acc -= e * Rl[herm_idx(t, u, v)];
-                                            else acc += e * Rl[herm_idx(t, u, v)];
-                                            ++c;
-                                        }
-                                Vr[s][f - f0] = acc;
-                            }
-                        }
-                    }
-                    team_sync<TW, TPB>();
                 }
                 // this chunk of V to shared memory
 #pragma unroll

@@ -12,6 +12,8 @@ configurations of the integral-direct Cholesky benchmark:
 * ``c4`` 20 atoms, 12 bohr cube, the c1 recipe (280 AOs); density X X^T with
   X ~ N(0, 0.1^2), 280 x 30.
 * ``c5`` 120 atoms, 24 bohr cube, the c2 recipe (3600 AOs), MO 150 x 2700.
+* ``c2s`` 12 atoms with the c2 recipe at the c2 atom density (360 AOs),
+  MO 18 x 270: the same kernels as c2 on a case small enough to profile.
 
 Atoms are placed uniformly in the cube and rejected when closer than
 1.7 bohr to an accepted atom; contraction coefficients are N(0, 1) before
@@ -80,6 +82,9 @@ def config(name: str, index: int = 0) -> Molecule:
         return random_molecule(1, 10, 8.0, RECIPE_C1, (3, 3), (0.1, 1e3), 1e-6, "c1")
     if name == "c2":
         return random_molecule(2, 40, 16.0, RECIPE_C2, (3, 6), (0.05, 5e3), 1e-6, "c2")
+    if name == "c2s":
+        # the c2 recipe at the c2 atom density with 12 atoms (360 AOs): profiling-size case
+        return random_molecule(2, 12, 16.0 * (12 / 40) ** (1 / 3), RECIPE_C2, (3, 6), (0.05, 5e3), 1e-6, "c2s")
     if name == "c3":
         counts = np.random.default_rng(3).integers(3, 31, 64)
         return random_molecule(3000 + index, int(counts[index]), 8.0, RECIPE_C1, (3, 3), (0.1, 1e3), 1e-5,
@@ -97,7 +102,7 @@ def mo_coefficients(nao: int, seed: int) -> np.ndarray:
     return np.asfortranarray(q * np.sign(np.diag(r)))
 
 
-MO_SPLIT = {"c1": (20, 60, 101), "c2": (60, 900, 102), "c5": (150, 2700, 105)}
+MO_SPLIT = {"c1": (20, 60, 101), "c2": (60, 900, 102), "c2s": (18, 270, 102), "c5": (150, 2700, 105)}
 
 
 def small_molecule(seed: int, natoms: int = 3, recipe=RECIPE_C1, cube: float = 5.0, nprim=(3, 3),
