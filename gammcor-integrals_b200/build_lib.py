@@ -23,7 +23,7 @@ NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-I", str(HERE.parent / "include"), "-I", str(CSRC)]
-SOURCES = ["eri_kernels.cu", "eri_classes_a.cu", "eri_classes_b.cu", "eri_classes_c.cu", "eri_classes_d.cu", "eri_kf_a.cu", "eri_kf_b.cu", "eri_kf_c.cu", "eri_kf_d.cu", "chol_kernels.cu", "mo_gemm.cu", "gci_api.cu", "host_math.cpp"]
+SOURCES = ["eri_kernels.cu", "eri_classes_a.cu", "eri_kf_a.cu", "eri_kf_b.cu", "eri_kf_c.cu", "eri_kf_d.cu", "chol_kernels.cu", "mo_gemm.cu", "gci_api.cu", "host_math.cpp"]
 HEADERS = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "gci.h"]
 
 

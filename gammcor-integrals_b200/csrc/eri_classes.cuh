@@ -33,16 +33,19 @@ static void launch_class(const EriArgs& args, cudaStream_t st)
     kern<<<(unsigned)blocks, G::TPB, smem, st>>>(args);
 }
 
-// Ket-first kernel (eri_ketfirst.cuh), built for bra types from (d,s) up:
-// a warp or a 128-thread block per quartet, grid capped at 64 blocks per SM
-// with a grid-stride loop inside.
-template <int TB, int TK>
+// Ket-first kernel (eri_ketfirst.cuh), built for bra types from (d,s) up in
+// three team widths (32, 64, 128 lanes per quartet); grid capped at 64 blocks
+// per SM with a grid-stride loop inside.
+constexpr int kNumKfWidths = 3;
+constexpr int kf_width(int w) { return w == 0 ? 32 : (w == 1 ? 64 : 128); }
+
+template <int TB, int TK, int TWQ>
 static void launch_kf(const EriArgs& args, cudaStream_t st)
 {
     constexpr int LA = type_lhi(TB), LB = type_llo(TB), LC = type_lhi(TK), LD = type_llo(TK);
-    using K = KfShape<LA, LB, LC, LD>;
+    using K = KfShape<LA, LB, LC, LD, TWQ>;
     const size_t smem = K::smem_bytes();
-    auto kern = k_eri_kf<LA, LB, LC, LD>;
+    auto kern = k_eri_kf<LA, LB, LC, LD, TWQ>;
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -56,13 +59,33 @@ static void launch_kf(const EriArgs& args, cudaStream_t st)
     kern<<<(unsigned)blocks, K::TPB, smem, st>>>(args);
 }
 
-constexpr bool has_kf(int tb, int tk) { return tb >= 3 && tk <= tb; }
-
-template <int TB, int TK = TB>
-static void register_row_kf(LaunchFn (*tab)[kNumPairTypes])
+// which widths are built: a warp only while a quartet's W block stays small,
+// 64 lanes up to 4096 elements, 128 lanes only from 512 elements; all within 227 KB
+template <int TB, int TK, int W>
+constexpr bool has_kf()
 {
-    if constexpr (has_kf(TB, TK)) tab[TB][TK] = &launch_kf<TB, TK>;
-    if constexpr (TK > 0) register_row_kf<TB, TK - 1>(tab);
+    if (TB < 3 || TK > TB) return false;
+    constexpr int LA = type_lhi(TB), LB = type_llo(TB), LC = type_lhi(TK), LD = type_llo(TK);
+    constexpr int nw = ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD);
+    if (W == 0 && nw > 4096) return false;
+    if (W == 1 && nw > 6000) return false;
+    if (W == 2 && nw < 512) return false;
+    return KfShape<LA, LB, LC, LD, kf_width(W)>::smem_bytes() <= 227 * 1024;
+}
+
+template <int TB, int W, int TK = TB>
+static void register_row_kf(LaunchFn (*tab)[kNumPairTypes][kNumPairTypes])
+{
+    if constexpr (has_kf<TB, TK, W>()) tab[W][TB][TK] = &launch_kf<TB, TK, kf_width(W)>;
+    if constexpr (TK > 0) register_row_kf<TB, W, TK - 1>(tab);
+}
+
+template <int TB>
+static void register_row_kf_all(LaunchFn (*tab)[kNumPairTypes][kNumPairTypes])
+{
+    register_row_kf<TB, 0>(tab);
+    register_row_kf<TB, 1>(tab);
+    register_row_kf<TB, 2>(tab);
 }
 
 // register the classes (TB, TK) for TK = 0..TB into a launch table
@@ -74,12 +97,9 @@ static void register_row(LaunchFn (*tab)[kNumPairTypes])
 }
 
 void register_eri_classes_a(LaunchFn (*tab)[kNumPairTypes]);
-void register_eri_classes_b(LaunchFn (*tab)[kNumPairTypes]);
-void register_eri_classes_c(LaunchFn (*tab)[kNumPairTypes]);
-void register_eri_classes_d(LaunchFn (*tab)[kNumPairTypes]);
-void register_eri_kf_a(LaunchFn (*tab)[kNumPairTypes]);
-void register_eri_kf_b(LaunchFn (*tab)[kNumPairTypes]);
-void register_eri_kf_c(LaunchFn (*tab)[kNumPairTypes]);
-void register_eri_kf_d(LaunchFn (*tab)[kNumPairTypes]);
+void register_eri_kf_a(LaunchFn (*tab)[kNumPairTypes][kNumPairTypes]);
+void register_eri_kf_b(LaunchFn (*tab)[kNumPairTypes][kNumPairTypes]);
+void register_eri_kf_c(LaunchFn (*tab)[kNumPairTypes][kNumPairTypes]);
+void register_eri_kf_d(LaunchFn (*tab)[kNumPairTypes][kNumPairTypes]);
 
 } // namespace gci

@@ -1,4 +1,6 @@
-// eri_classes_a.cu -- ERI class kernels with bra pair types [0, 1, 2, 3, 4, 5].
+// eri_classes_a.cu -- team ERI class kernels with bra pair types [0, 1, 2, 3, 4, 5]
+// (s, p and d bras).  Classes with an f shell in the bra use the ket-first
+// kernels only: the team kernel never won the per-class timing there.
 #include "eri_classes.cuh"
 
 namespace gci {

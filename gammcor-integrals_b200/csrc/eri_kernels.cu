@@ -101,27 +101,38 @@ __global__ void k_boys_eval(int m, int64_t n, const double* __restrict__ x, cons
     }
 }
 
-static LaunchFn g_launch[kNumPairTypes][kNumPairTypes];      // team kernels, every canonical class
-static LaunchFn g_launch_kf[kNumPairTypes][kNumPairTypes];   // ket-first kernels where built
-static int g_variant[kNumPairTypes][kNumPairTypes];          // 0 team, 1 ket-first
+static LaunchFn g_launch[kNumPairTypes][kNumPairTypes];                   // team kernels (bra types up to (d,d))
+static LaunchFn g_launch_kf[kNumKfWidths][kNumPairTypes][kNumPairTypes];  // ket-first kernels where built
+static int g_variant[kNumPairTypes][kNumPairTypes];   // 0 team, 1 + w ket-first of width kf_width(w)
+
+static LaunchFn variant_fn(int tb, int tk, int v)
+{
+    if (v == 0) return g_launch[tb][tk];
+    if (v >= 1 && v <= kNumKfWidths) return g_launch_kf[v - 1][tb][tk];
+    return nullptr;
+}
 
 cudaError_t eri_module_init()
 {
     static bool done = false;
     if (done) return cudaSuccess;
     register_eri_classes_a(g_launch);
-    register_eri_classes_b(g_launch);
-    register_eri_classes_c(g_launch);
-    register_eri_classes_d(g_launch);
     register_eri_kf_a(g_launch_kf);
     register_eri_kf_b(g_launch_kf);
     register_eri_kf_c(g_launch_kf);
     register_eri_kf_d(g_launch_kf);
+    // default before tuning: the narrowest ket-first kernel built, else the team kernel
     for (int tb = 0; tb < kNumPairTypes; ++tb)
-        for (int tk = 0; tk <= tb; ++tk) g_variant[tb][tk] = g_launch_kf[tb][tk] ? 1 : 0;
+        for (int tk = 0; tk <= tb; ++tk) {
+            g_variant[tb][tk] = 0;
+            for (int v = kNumKfWidths; v >= 1; --v)
+                if (variant_fn(tb, tk, v)) g_variant[tb][tk] = v;
+        }
     done = true;
     return cudaSuccess;
 }
+
+int eri_num_variants() { return 1 + kNumKfWidths; }
 
 int eri_variant(int tb, int tk)
 {
@@ -132,8 +143,7 @@ int eri_variant(int tb, int tk)
 int eri_set_variant(int tb, int tk, int variant)
 {
     if (tb < 0 || tk < 0 || tb >= kNumPairTypes || tk >= kNumPairTypes || tb < tk) return -1;
-    if (variant == 1 && !g_launch_kf[tb][tk]) return -1;
-    if (variant != 0 && variant != 1) return -1;
+    if (!variant_fn(tb, tk, variant)) return -1;
     g_variant[tb][tk] = variant;
     return 0;
 }
@@ -141,8 +151,7 @@ int eri_set_variant(int tb, int tk, int variant)
 cudaError_t eri_launch(int tb, int tk, const EriArgs& args, cudaStream_t st)
 {
     if (tb < 0 || tk < 0 || tb >= kNumPairTypes || tk >= kNumPairTypes || tb < tk) return cudaErrorInvalidValue;
-    LaunchFn fn = (g_variant[tb][tk] == 1) ? g_launch_kf[tb][tk] : g_launch[tb][tk];
-    fn(args, st);
+    variant_fn(tb, tk, g_variant[tb][tk])(args, st);
     count_launch();
     return cudaGetLastError();
 }

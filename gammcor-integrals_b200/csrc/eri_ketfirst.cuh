@@ -12,8 +12,8 @@
 // by one to two orders of magnitude; the bra products are applied once per
 // bra primitive pair.
 //
-// A team of TW lanes (one warp, or the whole 128-thread block when the W
-// block of a quartet is large) evaluates one quartet.  Lanes own bra Hermite
+// A team of TW lanes (one warp, or a whole block of 64 or 128 threads)
+// evaluates one quartet.  Lanes own bra Hermite
 // indices h in the primitive loop (V in registers, the ket pairs cd taken in
 // chunks that fit the register file; R is rebuilt per chunk) and elements of
 // W in the bra update (registers when they fit, shared memory otherwise).
@@ -40,12 +40,12 @@ GCI_HD constexpr int pair_prod_off(int lc, int ld, int f)
     return n;
 }
 
-template <int LA, int LB, int LC, int LD>
+// Team width TWQ: one warp (several teams per block) or a whole block of 64
+// or 128 threads per quartet; the autotuner picks the width per class.
+template <int LA, int LB, int LC, int LD, int TWQ>
 struct KfShape {
     using S = EriShape<LA, LB, LC, LD>;
-    // team width: the whole block (128 lanes) when W has more than 40
-    // elements per lane of a warp, else one warp
-    static constexpr int TW = (S::NE * S::NF > 40 * 32) ? 128 : 32;
+    static constexpr int TW = TWQ;
     static constexpr int SLOTS = (S::H1 + TW - 1) / TW;        // bra Hermite indices per lane
     static constexpr int WSLOTS = (S::NE * S::NF + TW - 1) / TW;
     static constexpr bool WREG = WSLOTS <= 40;                 // W in registers, else shared memory
@@ -72,22 +72,22 @@ struct KfShape {
     // of h + g; Hermite index of every bra product; first bra product of each ab
     static constexpr int TAB_INTS = S::HT + S::H2 * S::H1 + S::NCB + S::NE + 1;
     // teams per block: four warps while their scratch stays within 160 KB
-    static constexpr int TEAMS = TW == 128 ? 1
-                                           : ((size_t)SZ * 8 * 4 <= 160 * 1024 ? 4
-                                                                               : ((size_t)SZ * 8 * 2 <= 200 * 1024 ? 2 : 1));
-    static constexpr int TPB = TW == 128 ? 128 : 32 * TEAMS;
+    static constexpr int TEAMS = TW > 32 ? 1
+                                         : ((size_t)SZ * 8 * 4 <= 160 * 1024 ? 4
+                                                                             : ((size_t)SZ * 8 * 2 <= 200 * 1024 ? 2 : 1));
+    static constexpr int TPB = TW > 32 ? TW : 32 * TEAMS;
     static constexpr size_t smem_bytes()
     {
         return sizeof(double) * ((size_t)TEAMS * SZ + S::HT) + sizeof(int) * (size_t)TAB_INTS;
     }
 };
 
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(KfShape<LA, LB, LC, LD>::TPB)
+template <int LA, int LB, int LC, int LD, int TWQ>
+__global__ void __launch_bounds__(KfShape<LA, LB, LC, LD, TWQ>::TPB)
 k_eri_kf(const EriArgs a)
 {
     using S = EriShape<LA, LB, LC, LD>;
-    using K = KfShape<LA, LB, LC, LD>;
+    using K = KfShape<LA, LB, LC, LD, TWQ>;
     constexpr int TW = K::TW, TPB = K::TPB;
     extern __shared__ double smem[];
     double* tab_coef = smem + (size_t)K::TEAMS * K::SZ;           // recursion coefficient of h

@@ -2,10 +2,10 @@
 #include "eri_classes.cuh"
 
 namespace gci {
-void register_eri_kf_a(LaunchFn (*tab)[kNumPairTypes])
+void register_eri_kf_a(LaunchFn (*tab)[kNumPairTypes][kNumPairTypes])
 {
-    register_row_kf<3>(tab);
-    register_row_kf<4>(tab);
-    register_row_kf<5>(tab);
+    register_row_kf_all<3>(tab);
+    register_row_kf_all<4>(tab);
+    register_row_kf_all<5>(tab);
 }
 } // namespace gci

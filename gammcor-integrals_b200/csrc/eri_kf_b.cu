@@ -2,9 +2,9 @@
 #include "eri_classes.cuh"
 
 namespace gci {
-void register_eri_kf_b(LaunchFn (*tab)[kNumPairTypes])
+void register_eri_kf_b(LaunchFn (*tab)[kNumPairTypes][kNumPairTypes])
 {
-    register_row_kf<6>(tab);
-    register_row_kf<7>(tab);
+    register_row_kf_all<6>(tab);
+    register_row_kf_all<7>(tab);
 }
 } // namespace gci

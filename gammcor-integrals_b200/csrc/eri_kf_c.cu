@@ -2,8 +2,8 @@
 #include "eri_classes.cuh"
 
 namespace gci {
-void register_eri_kf_c(LaunchFn (*tab)[kNumPairTypes])
+void register_eri_kf_c(LaunchFn (*tab)[kNumPairTypes][kNumPairTypes])
 {
-    register_row_kf<8>(tab);
+    register_row_kf_all<8>(tab);
 }
 } // namespace gci

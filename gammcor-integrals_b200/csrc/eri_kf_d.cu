@@ -2,8 +2,8 @@
 #include "eri_classes.cuh"
 
 namespace gci {
-void register_eri_kf_d(LaunchFn (*tab)[kNumPairTypes])
+void register_eri_kf_d(LaunchFn (*tab)[kNumPairTypes][kNumPairTypes])
 {
-    register_row_kf<9>(tab);
+    register_row_kf_all<9>(tab);
 }
 } // namespace gci

@@ -330,7 +330,10 @@ struct Handle {
     double t_rkpq = 0.0, t_rkab = 0.0;
     // work counters: GEMM flops per phase and ERI work per canonical class
     double gemm_flops[kNumGemm] = {0};
-    double eri_stats[kNumPairTypes][kNumPairTypes][4] = {};   // quartets, prim quartets evaluated, integrals, prim quartets unscreened
+    // per canonical class: quartets, primitive quartets after the pair screen, integrals, primitive
+    // quartets before it, bra primitive pairs x quartets, ket primitive pairs x quartets
+    static constexpr int kNumStats = 6;
+    double eri_stats[kNumPairTypes][kNumPairTypes][kNumStats] = {};
     // scratch reused across ERI launches
     DVec<int> d_bra, d_ket;
 };
@@ -507,6 +510,8 @@ static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<in
             H.eri_stats[tb][tb][1] += np2;
             H.eri_stats[tb][tb][2] += nf2;
             H.eri_stats[tb][tb][3] += nu2;
+            H.eri_stats[tb][tb][4] += npb;
+            H.eri_stats[tb][tb][5] += npb;
             a.bra_ids = H.d_bra.p + sb[tb];
             a.ket_ids = a.bra_ids;
             a.nbra = nb;
@@ -525,6 +530,9 @@ static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<in
             H.eri_stats[cb][ck][1] += npb * npk;
             H.eri_stats[cb][ck][2] += nfb * nfk;
             H.eri_stats[cb][ck][3] += nub * nuk;
+            // primitives of the canonical bra / ket side times the quartets they enter
+            H.eri_stats[cb][ck][4] += tb >= tk ? npb * (double)nk : npk * (double)nb;
+            H.eri_stats[cb][ck][5] += tb >= tk ? npk * (double)nb : npb * (double)nk;
             a.bra_ids = H.d_bra.p + sb[tb];
             a.ket_ids = H.d_ket.p + sk[tk];
             a.nbra = nb;
@@ -1354,12 +1362,13 @@ int gci_stats(const gci_handle* h, double* out, int n)
 {
     if (!h || !out) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
     const Handle& H = h->h;
-    std::vector<double> v(8 + 4 * kNumPairTypes * kNumPairTypes, 0.0);
+    constexpr int ns = Handle::kNumStats;
+    std::vector<double> v(8 + ns * kNumPairTypes * kNumPairTypes, 0.0);
     for (int i = 0; i < kNumGemm; ++i) v[i] = H.gemm_flops[i];
     for (int tb = 0; tb < kNumPairTypes; ++tb)
         for (int tk = 0; tk < kNumPairTypes; ++tk)
-            for (int q = 0; q < 4; ++q) {
-                v[8 + 4 * (tb * kNumPairTypes + tk) + q] = H.eri_stats[tb][tk][q];
+            for (int q = 0; q < ns; ++q) {
+                v[8 + ns * (tb * kNumPairTypes + tk) + q] = H.eri_stats[tb][tk][q];
                 if (q < 3) v[5 + q] += H.eri_stats[tb][tk][q];
             }
     for (int i = 0; i < n && i < (int)v.size(); ++i) out[i] = v[i];
@@ -1511,20 +1520,34 @@ int gci_autotune_eri(const gci_basis* basis, int max_pairs, double* seconds)
         cudaEvent_t e0, e1;
         CU(cudaEventCreate(&e0));
         CU(cudaEventCreate(&e1));
-        std::vector<double> times((size_t)kNumPairTypes * kNumPairTypes * 2, 0.0);
+        const int kVariants = eri_num_variants();
+        std::vector<double> times((size_t)kNumPairTypes * kNumPairTypes * kVariants, 0.0);
         try {
             for (int tb = 0; tb < kNumPairTypes; ++tb)
                 for (int tk = 0; tk <= tb; ++tk) {
                     if (by_type[tb].empty() || by_type[tk].empty()) continue;
                     const int keep = eri_variant(tb, tk);
-                    if (eri_set_variant(tb, tk, 1) != 0) continue;   // one kernel only: nothing to choose
+                    int navail = 0;
+                    for (int v = 0; v < kVariants; ++v)
+                        if (eri_set_variant(tb, tk, v) == 0) ++navail;
                     eri_set_variant(tb, tk, keep);
-                    double best[2] = {-1.0, -1.0};
-                    for (int v = 0; v < 2; ++v) {
+                    if (navail < 2) continue;   // one kernel only: nothing to choose
+                    std::vector<double> best(kVariants, -1.0);
+                    for (int v = 0; v < kVariants; ++v) {
                         if (eri_set_variant(tb, tk, v) != 0) continue;
-                        run_eri(H, by_type[tb], by_type[tk], kModeProduct, &m, &m, out.p, kSide);   // warm-up
                         float ms = 0.0f, msmin = 1e30f;
-                        for (int rep = 0; rep < 2; ++rep) {
+                        // warm-up, timed too: a variant three times slower than the best so far is not repeated
+                        CU(cudaEventRecord(e0, C.stream));
+                        run_eri(H, by_type[tb], by_type[tk], kModeProduct, &m, &m, out.p, kSide);
+                        CU(cudaEventRecord(e1, C.stream));
+                        CU(cudaEventSynchronize(e1));
+                        CU(cudaEventElapsedTime(&ms, e0, e1));
+                        double bestv = -1.0;
+                        for (int u = 0; u < v; ++u)
+                            if (best[u] >= 0.0 && (bestv < 0.0 || best[u] < bestv)) bestv = best[u];
+                        const int reps = (bestv >= 0.0 && 1e-3 * ms > 3.0 * bestv) ? 0 : 2;
+                        if (reps == 0) msmin = ms;
+                        for (int rep = 0; rep < reps; ++rep) {
                             CU(cudaEventRecord(e0, C.stream));
                             run_eri(H, by_type[tb], by_type[tk], kModeProduct, &m, &m, out.p, kSide);
                             CU(cudaEventRecord(e1, C.stream));
@@ -1533,11 +1556,11 @@ int gci_autotune_eri(const gci_basis* basis, int max_pairs, double* seconds)
                             msmin = std::min(msmin, ms);
                         }
                         best[v] = 1e-3 * msmin;
-                        times[((size_t)tb * kNumPairTypes + tk) * 2 + v] = best[v];
+                        times[((size_t)tb * kNumPairTypes + tk) * kVariants + v] = best[v];
                     }
                     int pick = keep;
-                    if (best[0] >= 0.0 && best[1] >= 0.0) pick = best[1] < best[0] ? 1 : 0;
-                    else if (best[0] >= 0.0) pick = 0;
+                    for (int v = 0; v < kVariants; ++v)
+                        if (best[v] >= 0.0 && (best[pick] < 0.0 || best[v] < best[pick])) pick = v;
                     eri_set_variant(tb, tk, pick);
                 }
         } catch (...) {

@@ -10,8 +10,10 @@ int64_t launches();
 
 cudaError_t eri_module_init();
 cudaError_t eri_launch(int tb, int tk, const EriArgs& args, cudaStream_t st);
-// Kernel variant of the canonical class (tb, tk): 0 team kernel, 1 ket-first
-// warp kernel (only where built); eri_set_variant returns -1 when unavailable.
+// Kernel variant of the canonical class (tb, tk): 0 team kernel, 1..3
+// ket-first kernel with 32, 64 or 128 lanes per quartet (only where built);
+// eri_set_variant returns -1 when unavailable.
+int eri_num_variants();
 int eri_variant(int tb, int tk);
 int eri_set_variant(int tb, int tk, int variant);
 cudaError_t pair_records_launch(const ShellPairDev* pairs, int npairs, const double* xyz, const int* poff,

@@ -68,11 +68,12 @@ def class_flops(la, lb, lc, ld, spher=True):
     return prim, epi
 
 
-# Counter layouts: the library (gci_stats) keeps 4 counters per class over
-# 10 pair types -- quartets, primitive quartets evaluated, integrals, primitive
-# quartets before the primitive-pair screen; the oracle (orc_stats) keeps 3
+# Counter layouts: the library (gci_stats) keeps 6 counters per class over
+# 10 pair types -- quartets, primitive quartets after the primitive-pair
+# screen, integrals, primitive quartets before it, bra primitive pairs x
+# quartets, ket primitive pairs x quartets; the oracle (orc_stats) keeps 3
 # per class over 21 pair types and evaluates every primitive quartet.
-LAYOUTS = {"lib": (10, 4), "oracle": (21, 3)}
+LAYOUTS = {"lib": (10, 6), "oracle": (21, 3)}
 
 
 def eri_flops(stats: np.ndarray, layout: str, spher=True, unscreened=False) -> float:
@@ -80,7 +81,7 @@ def eri_flops(stats: np.ndarray, layout: str, spher=True, unscreened=False) -> f
     quartets the reference algorithm evaluates (no primitive screening)."""
     ntypes, nc = LAYOUTS[layout]
     types = pair_types({10: 3, 21: 5}[ntypes])
-    col = 3 if (unscreened and nc == 4) else 1
+    col = 3 if (unscreened and nc == 6) else 1
     total = 0.0
     for tb in range(ntypes):
         for tk in range(ntypes):
@@ -103,3 +104,49 @@ def job_flops(stats: np.ndarray, layout: str, spher=True) -> dict:
     return {"gemm": gemm, "eri": eri_ref, "eri_executed": eri_run, "total": gemm + eri_ref,
             "executed": gemm + eri_run, "integrals": float(stats[7]), "quartets": float(stats[5]),
             "prim_quartets": float(stats[6])}
+
+
+def pair_supp_sum(la, lb):
+    """Hermite products of all Cartesian pairs of shells (la, lb) (two-centre form)."""
+    return sum((ax + bx + 1) * (ay + by + 1) * (az + bz + 1) for ax, ay, az in carts(la) for bx, by, bz in carts(lb))
+
+
+@lru_cache(maxsize=None)
+def kernel_class_flops(la, lb, lc, ld, variant, spher=True):
+    """Arithmetic of this library's kernels for one class: (per primitive quartet,
+    per bra primitive pair x quartet, per ket primitive pair x quartet, per quartet).
+    variant 0: bra-first team kernel; 1..3: ket-first kernel (any team width)."""
+    L1, L2 = la + lb, lc + ld
+    LT = L1 + L2
+    H1, H2 = herm_n(L1), herm_n(L2)
+    ncb, nck = pair_supp_sum(la, lb), pair_supp_sum(lc, ld)
+    nA, nB, nC, nD = ncart(la), ncart(lb), ncart(lc), ncart(ld)
+    NE, NF = nA * nB, nC * nD
+    boys = 30 + 3 * LT
+    pref = 25
+    rrec = 3 * sum(herm_n(n) for n in range(1, LT + 1))
+    nf = (lambda l: 2 * l + 1) if spher else ncart
+    fA, fB, fC, fD = nf(la), nf(lb), nf(lc), nf(ld)
+    epi = 2 * NE * nC * fD * nD + 2 * NE * fC * fD * nC + 2 * nA * fB * fC * fD * nB + 2 * fA * fB * fC * fD * nA
+    if variant == 0:
+        return boys + pref + rrec + 2 * ncb * H2, 0, 2 * NE * nck, epi
+    return boys + pref + rrec + 2 * H1 * nck, 2 * ncb * NF, 0, epi
+
+
+def kernel_flops(stats: np.ndarray, variants: dict, spher=True) -> float:
+    """FP64 arithmetic the library's ERI kernels executed, from gci_stats counters and the
+    kernel variant of each class ({(tb, tk): variant})."""
+    ntypes, nc = LAYOUTS["lib"]
+    types = pair_types(3)
+    total = 0.0
+    for tb in range(ntypes):
+        for tk in range(ntypes):
+            base = 8 + nc * (tb * ntypes + tk)
+            q = stats[base]
+            if q == 0:
+                continue
+            pq, nbp, nkp = stats[base + 1], stats[base + 4], stats[base + 5]
+            (la, lb), (lc, ld) = types[tb], types[tk]
+            prim, perb, perk, epi = kernel_class_flops(la, lb, lc, ld, variants.get((tb, tk), 0), spher)
+            total += pq * prim + nbp * perb + nkp * perk + q * epi
+    return total

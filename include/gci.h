@@ -118,9 +118,11 @@ int gci_rkab_device(gci_handle *h, const double *CA, int64_t ldca, int64_t a0, i
 
 /* Work done on this handle: [0..4] GEMM flops of M-LL^T, new vectors, potrf+trtri, Inv_L
  * products, AO->MO; [5] shell quartets, [6] primitive quartets, [7] integrals evaluated;
- * then per canonical class (bra type, ket type) of 10 x 10 pair types: quartets,
- * primitive quartets evaluated, integrals, primitive quartets before the primitive-pair
- * screen.  Pair type of (l_hi, l_lo) = l_hi(l_hi+1)/2 + l_lo. */
+ * then per canonical class (bra type, ket type) of 10 x 10 pair types, 6 counters:
+ * quartets, primitive quartets after the primitive-pair screen, integrals, primitive
+ * quartets before that screen, bra primitive pairs x quartets, ket primitive pairs x
+ * quartets.
+ * Pair type of (l_hi, l_lo) = l_hi(l_hi+1)/2 + l_lo. */
 int gci_stats(const gci_handle *h, double *out, int n);
 
 /* Kernels of this library launched so far in the process (cuBLAS/cuSOLVER calls excluded). */
@@ -162,16 +164,17 @@ int gci_eri_pairs(const gci_basis *basis, double omega, double *out, int64_t ld)
 
 /* Each ERI class (pair types tb >= tk, pair type = lhi*(lhi+1)/2 + llo of the
  * two shells' angular momenta) has a team kernel (variant 0: lanes over the
- * ket Hermite indices, every class) and, for bra types from (d,s) up and ket
- * types up to (f,p), a ket-first warp kernel (variant 1).
- * gci_eri_variant(tb, tk, v): v = 0 or 1 selects, v < 0 only queries; returns
- * the variant in use (>= 0) or GCI_ERR_ARG.  The choice is process-wide. */
+ * ket Hermite indices; bra types up to (d,d)) and, for bra types from (d,s) up,
+ * ket-first kernels with 32, 64 or 128 lanes per quartet (variants 1, 2, 3,
+ * where built).  gci_eri_variant(tb, tk, v): v >= 0 selects, v < 0 only
+ * queries; returns the variant in use (>= 0) or GCI_ERR_ARG.  The choice is
+ * process-wide. */
 int gci_eri_variant(int tb, int tk, int variant);
 
-/* Autotuner: times both variants of every class that occurs in `basis` on a
+/* Autotuner: times every variant of every class that occurs in `basis` on a
  * product-mode sample of its shell pairs (up to max_pairs bra and max_pairs
- * ket pairs per class) with CUDA events and keeps the faster one.  If
- * `seconds` is not NULL it receives 10 x 10 x 2 launch times (tb, tk,
+ * ket pairs per class) with CUDA events and keeps the fastest.  If
+ * `seconds` is not NULL it receives 10 x 10 x 4 launch times (tb, tk,
  * variant; 0 where not measured). */
 int gci_autotune_eri(const gci_basis *basis, int max_pairs, double *seconds);
 
