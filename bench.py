@@ -194,6 +194,98 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_grad(args, rank, world, local):
+    """c4: Coulomb energy and nuclear gradient of D = X X^T (X ~ N(0, 0.1^2), 280 x 30, seed 104)
+    through the adjoint kernels (gci_coulomb_grad_device; e2e through gci_coulomb_grad)."""
+    import torch
+    import gammcor_pkg
+    gammcor_pkg.load()
+    from gammcor_integrals_b200 import _capi, basis, flops, molecules
+    L = _capi.lib()
+    _capi.check(L.gci_init())
+    mol = molecules.config("c4")
+    tb = basis.from_molecule(mol)
+    nao = tb.NAO
+    X = np.random.default_rng(104).normal(0.0, 0.1, (nao, 30))
+    Dm = X @ X.T
+    Dd = torch.from_numpy(Dm).cuda()
+    sptr = C.c_void_p()
+    _capi.check(L.gci_get_stream(C.byref(sptr)))
+    lib_stream = torch.cuda.ExternalStream(sptr.value)
+    s = tb.c_struct()
+    e = C.c_double()
+    g = np.zeros((tb.NAtoms, 3))
+
+    def step():
+        _capi.check(L.gci_coulomb_grad_device(C.byref(s), 0.0, C.c_void_p(Dd.data_ptr()), nao, C.byref(e),
+                                              _capi.ptr(g), None, nao))
+
+    for _ in range(args.warmup):
+        step()
+    work = np.zeros(49)
+    _capi.check(L.gci_coulomb_grad_work(_capi.ptr(work), 49))
+    fl = flops.grad_flops(work)
+    n0 = C.c_int64()
+    _capi.check(L.gci_kernel_launches(C.byref(n0)))
+    flush = torch.empty(64 << 20, dtype=torch.float64, device="cuda")
+    t = 0.0
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            with torch.cuda.stream(lib_stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(lib_stream)
+            step()
+            e1.record(lib_stream)
+            e1.synchronize()
+            t += e0.elapsed_time(e1) * 1e-3
+        torch.cuda.synchronize()
+    n1 = C.c_int64()
+    _capi.check(L.gci_kernel_launches(C.byref(n1)))
+    # end to end: density from pinned host memory, gradient and energy back to the host
+    pin = torch.from_numpy(Dm).pin_memory()
+    te0, te1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    te0.record(lib_stream)
+    for _ in range(max(1, args.e2e_steps)):
+        _capi.check(L.gci_coulomb_grad(C.byref(s), 0.0, _capi.ptr(pin.numpy()), nao, C.byref(e), _capi.ptr(g),
+                                       None, nao))
+    te1.record(lib_stream)
+    te1.synchronize()
+    te = te0.elapsed_time(te1) * 1e-3 / max(1, args.e2e_steps)
+    peak64 = measured_fp64_peak(torch)
+    rate = fl / (t / args.steps) / 1e12
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        sub = molecules.Molecule(atoms=mol.atoms[:3], shells=[sh for sh in mol.shells if sh[0] < 3])
+        ob = O.make_basis(sub.atoms, sub.shells)
+        Xs = X[:ob.nao]
+        t0 = time.perf_counter()
+        O.coulomb_energy_grad(ob, Xs @ Xs.T)
+        dt = time.perf_counter() - t0
+        scale = (len(mol.shells) / len(sub.shells)) ** 4     # the oracle loops over every ordered shell quartet
+        cpu = {"value": 1.0 / (dt * scale), "unit": "gradients/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"oracle (orc_coulomb_energy_grad, OpenMP) on the first 3 atoms of c4 "
+                         f"({len(sub.shells)} shells) in {dt:.2f} s, extrapolated by (120/{len(sub.shells)})^4 "
+                         f"shell quartets"}
+    line = {"metric": "c4 Coulomb energy + nuclear gradient (adjoint kernels)", "value": args.steps / t,
+            "unit": "gradients/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"c4: 20 atoms, NAO={nao}, D = X X^T (X 280 x 30)",
+                       "l2": "flushed before every timed step (512 MB write outside the timed events)"},
+            "energy": e.value, "gflop_per_step": fl / 1e9, "primitive_quartets": float(work.sum()),
+            "gpu_launches": int(n1.value - n0.value),
+            "roofline": {"bound": "fp64", "kernel": "k_grad_potential (all level classes) + set-up",
+                         "achieved": rate, "peak": peak64, "unit": "TFLOP/s", "frac": rate / peak64,
+                         "traffic": None, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"},
+            "e2e": {"value": 1.0 / te, "unit": "gradients/s", "h2d_bytes_per_step": int(Dm.nbytes),
+                    "d2h_bytes_per_step": int(g.nbytes + 8)},
+            "clocks": clk.summary(), "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -201,6 +293,12 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.config == "c4":
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            run_grad(args, rank, world, local)
         return
     import torch
     import torch.distributed as dist

@@ -23,19 +23,41 @@ NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-I", str(HERE.parent / "include"), "-I", str(CSRC)]
-SOURCES = ["eri_kernels.cu", "eri_classes_a.cu", "eri_kf_a.cu", "eri_kf_b.cu", "eri_kf_c.cu", "eri_kf_d.cu", "chol_kernels.cu", "mo_gemm.cu", "gci_api.cu", "host_math.cpp"]
+SOURCES = ["eri_kernels.cu", "eri_classes_a.cu", "eri_kf_a.cu", "eri_kf_b.cu", "eri_kf_c.cu", "eri_kf_d.cu",
+           "grad_kernels.cu", "grad_pot_a.cu", "grad_pot_b.cu", "grad_pot_c.cu",
+           "chol_kernels.cu", "mo_gemm.cu", "gci_api.cu", "host_math.cpp"]
+# ptxas at -O3 keeps the largest unrolled potential kernels (level sums >= 8)
+# entirely in local memory; -O1 allocates registers for them
+EXTRA = {"grad_pot_b.cu": ["-Xptxas", "-O1"], "grad_pot_c.cu": ["-Xptxas", "-O1"]}
 HEADERS = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "gci.h"]
+
+
+def _deps(src: Path, seen=None) -> set:
+    """Local headers a source includes, transitively (#include "...")."""
+    seen = set() if seen is None else seen
+    for line in src.read_text().splitlines():
+        line = line.strip()
+        if line.startswith("#include \""):
+            name = line.split('"')[1]
+            for d in (src.parent, CSRC, HERE.parent / "include"):
+                h = (d / name).resolve()
+                if h.exists():
+                    if h not in seen:
+                        seen.add(h)
+                        _deps(h, seen)
+                    break
+    return seen
 
 
 def _stale(src: Path, obj: Path) -> bool:
     if not obj.exists():
         return True
     t = obj.stat().st_mtime
-    return src.stat().st_mtime > t or any(h.stat().st_mtime > t for h in HEADERS)
+    return src.stat().st_mtime > t or any(h.stat().st_mtime > t for h in _deps(src))
 
 
 def _compile(src: Path, obj: Path, verbose: bool) -> None:
-    cmd = [NVCC, *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
+    cmd = [NVCC, *ARCH, *COMMON, *EXTRA.get(src.name, []), "-c", str(src), "-o", str(obj)]
     if src.suffix == ".cpp":
         cmd = [NVCC, *COMMON, "-x", "c++", "-c", str(src), "-o", str(obj)]
     if verbose:

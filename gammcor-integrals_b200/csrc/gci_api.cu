@@ -1234,6 +1234,136 @@ struct gci_handle {
     Handle h;
 };
 
+// ------------------------------------------------------------------ adjoint: Coulomb energy and gradient
+// Work of the last gci_coulomb_grad call: primitive quartets per (bra level, ket level).
+static double g_grad_work[kGradMaxL + 1][kGradMaxL + 1];
+
+// J = 1/2 sum D_pq (pq|rs) D_rs, dJ/dAtomCoords and (optionally) the Coulomb
+// matrix, by the Hermite-vector scheme of grad_engine.cuh.  `dev` says whether
+// D and jmat are device pointers; energy and grad are host pointers.
+static void coulomb_grad_impl(const gci_basis* basis, double omega, const double* D, int64_t ldd, bool dev,
+                              double* energy, double* grad, double* jmat, int64_t ldj)
+{
+    if (!D) fail(GCI_ERR_ARG, "D is NULL");
+    if (!energy && !grad && !jmat) fail(GCI_ERR_ARG, "nothing requested");
+    Context& C = ctx();
+    CU(grad_module_init());
+    Handle H;
+    H.timer.s = C.stream;
+    H.kappa = (omega > 0.0) ? 1.0 / (omega * omega) : 0.0;
+    H.hb = make_basis(basis);
+    const int64_t nao = H.hb.nao;
+    if (ldd < nao) fail(GCI_ERR_ARG, "leading dimension of D too small");
+    if (jmat && ldj < nao) fail(GCI_ERR_ARG, "leading dimension of jmat too small");
+    setup_pairs(H);
+    const PairTable& P = H.pt;
+    const HostBasis& hb = H.hb;
+    // primitive pairs grouped by Hermite level L = l1 + l2 of their shell pair
+    constexpr int NL = kGradMaxL + 1;
+    std::vector<int> lbeg(NL, 0), ln(NL, 0);
+    for (int64_t sp = 0; sp < P.n; ++sp) ln[P.h[sp].l1 + P.h[sp].l2] += P.h[sp].npp;
+    std::vector<int64_t> vec_off(NL, 0), hk_off(NL, 0), pot_off(NL, 0);
+    int64_t ntot = 0, nvec = 0, nhk = 0, npot = 0;
+    for (int L = 0; L < NL; ++L) {
+        lbeg[L] = (int)ntot;
+        vec_off[L] = nvec;
+        hk_off[L] = nhk;
+        pot_off[L] = npot;
+        ntot += ln[L];
+        nvec += (int64_t)ln[L] * kGradVec * grad_hb(L);
+        nhk += (int64_t)ln[L] * herm_n(L);
+        npot += (int64_t)ln[L] * grad_hb(L);
+    }
+    std::vector<int64_t> gbase(P.n);
+    std::vector<int> gpair(std::max<int64_t>(ntot, 1), 0);
+    {
+        std::vector<int64_t> run(lbeg.begin(), lbeg.end());
+        for (int64_t sp = 0; sp < P.n; ++sp) {
+            const int L = P.h[sp].l1 + P.h[sp].l2;
+            gbase[sp] = run[L];
+            for (int i = 0; i < P.h[sp].npp; ++i) gpair[run[L] + i] = (int)sp;
+            run[L] += P.h[sp].npp;
+        }
+    }
+    DVec<int64_t> d_gbase, d_voff, d_hkoff, d_potoff;
+    DVec<int> d_lbeg, d_ln, d_ppair;
+    DVec<double> mP, mX, mY, mZ, vecs, hk, V, dots, Dd, Jd;
+    d_gbase.upload(gbase, C.stream);
+    d_voff.upload(vec_off, C.stream);
+    d_hkoff.upload(hk_off, C.stream);
+    d_potoff.upload(pot_off, C.stream);
+    d_lbeg.upload(lbeg, C.stream);
+    d_ln.upload(ln, C.stream);
+    const size_t n1 = (size_t)std::max<int64_t>(ntot, 1);
+    mP.alloc(n1); mX.alloc(n1); mY.alloc(n1); mZ.alloc(n1);
+    d_ppair.alloc(n1);
+    vecs.alloc((size_t)std::max<int64_t>(nvec, 1));
+    hk.alloc((size_t)std::max<int64_t>(nhk, 1));
+    V.alloc((size_t)std::max<int64_t>(npot, 1));
+    dots.alloc(n1 * kGradVec);
+    const double* Dp = D;
+    if (!dev) {
+        Dd.alloc((size_t)ldd * nao);
+        CU(cudaMemcpyAsync(Dd.p, D, sizeof(double) * (size_t)ldd * nao, cudaMemcpyHostToDevice, C.stream));
+        Dp = Dd.p;
+    }
+    const DevBasis& db = H.db;
+    CU(grad_pair_vectors_launch(P.d.p, (int)P.n, d_gbase.p, d_lbeg.p, d_ln.p, d_voff.p, d_hkoff.p, db.xyz.p, db.poff.p,
+                                db.exps.p, db.coefs.p, P.plist.p, db.tmat.p, db.toff.p, db.nfunc.p, db.loc.p, Dp, ldd,
+                                mP.p, mX.p, mY.p, mZ.p, vecs.p, hk.p, d_ppair.p, C.stream));
+    CU(cudaMemsetAsync(V.p, 0, sizeof(double) * V.n, C.stream));
+    constexpr int64_t kChunk = 512;   // ket primitive pairs per warp
+    for (int L1 = 0; L1 < NL; ++L1)
+        for (int L2 = 0; L2 < NL; ++L2) {
+            g_grad_work[L1][L2] = (double)ln[L1] * (double)ln[L2];
+            if (ln[L1] == 0 || ln[L2] == 0) continue;
+            GradPotArgs a{};
+            a.mP = mP.p; a.mX = mX.p; a.mY = mY.p; a.mZ = mZ.p;
+            a.bra_beg = lbeg[L1]; a.nbra = ln[L1];
+            a.ket_beg = lbeg[L2]; a.nket = ln[L2];
+            a.hk = hk.p + hk_off[L2];
+            a.V = V.p + pot_off[L1];
+            a.chunk = kChunk;
+            a.nchunk = (ln[L2] + kChunk - 1) / kChunk;
+            a.kappa = H.kappa;
+            a.boys = C.boys.p;
+            CU(grad_potential_launch(L1, L2, a, C.stream));
+        }
+    for (int L = 0; L < NL; ++L)
+        CU(grad_dots_launch(lbeg[L], ln[L], grad_hb(L), vecs.p + vec_off[L], V.p + pot_off[L], dots.p, C.stream));
+    if (jmat) {
+        double* Jp = jmat;
+        if (!dev) {
+            Jd.alloc((size_t)ldj * nao);
+            Jp = Jd.p;
+        }
+        CU(grad_coulomb_matrix_launch(P.d.p, (int)P.n, d_gbase.p, d_lbeg.p, d_potoff.p, V.p, P.pp.p, db.tmat.p,
+                                      db.toff.p, db.nfunc.p, db.loc.p, Jp, ldj, C.stream));
+        if (!dev)
+            CU(cudaMemcpyAsync(jmat, Jd.p, sizeof(double) * (size_t)ldj * nao, cudaMemcpyDeviceToHost, C.stream));
+    }
+    std::vector<double> hd((size_t)n1 * kGradVec, 0.0);
+    if (ntot > 0)
+        CU(cudaMemcpyAsync(hd.data(), dots.p, sizeof(double) * (size_t)ntot * kGradVec, cudaMemcpyDeviceToHost,
+                           C.stream));
+    CU(cudaStreamSynchronize(C.stream));
+    // fixed-order host reduction: deterministic energy and gradient
+    double e = 0.0;
+    std::vector<double> g((size_t)3 * basis->natoms, 0.0);
+    for (int64_t i = 0; i < ntot; ++i) {
+        const ShellPairDev& sp = P.h[gpair[i]];
+        const double* d = &hd[(size_t)i * kGradVec];
+        e += 0.5 * d[0];
+        const int a1 = hb.atom[sp.s1], a2 = hb.atom[sp.s2];
+        for (int x = 0; x < 3; ++x) {
+            g[3 * a1 + x] += d[1 + x];
+            g[3 * a2 + x] += d[4 + x];
+        }
+    }
+    if (energy) *energy = e;
+    if (grad) std::copy(g.begin(), g.end(), grad);
+}
+
 extern "C" {
 
 int gci_init(void)
@@ -1677,6 +1807,26 @@ int gci_eri_pairs_noalloc(const gci_basis* basis, double omega, double* out_dev,
         CU(cudaStreamSynchronize(s));
         if (herr != 0) fail(GCI_ERR_CUDA, "ERI kernel reported error " + std::to_string(herr));
     });
+}
+
+int gci_coulomb_grad(const gci_basis* basis, double omega, const double* D, int64_t ldd, double* energy,
+                     double* grad, double* jmat, int64_t ldj)
+{
+    return guarded([&] { coulomb_grad_impl(basis, omega, D, ldd, false, energy, grad, jmat, ldj); });
+}
+
+int gci_coulomb_grad_device(const gci_basis* basis, double omega, const double* D_dev, int64_t ldd, double* energy,
+                            double* grad, double* jmat_dev, int64_t ldj)
+{
+    return guarded([&] { coulomb_grad_impl(basis, omega, D_dev, ldd, true, energy, grad, jmat_dev, ldj); });
+}
+
+int gci_coulomb_grad_work(double* out, int n)
+{
+    if (!out) { g_last_error = "out is NULL"; return GCI_ERR_ARG; }
+    const int m = (kGradMaxL + 1) * (kGradMaxL + 1);
+    for (int i = 0; i < n && i < m; ++i) out[i] = g_grad_work[i / (kGradMaxL + 1)][i % (kGradMaxL + 1)];
+    return GCI_OK;
 }
 
 } // extern "C"

@@ -135,4 +135,26 @@ struct EriArgs {
     int* err;                 // device error word
 };
 
+// ------------------------------------------------------------ adjoint (Coulomb gradient) path
+// Hermite level L of a shell pair (lA + lB) runs to 2 kMaxL; the derivative
+// vectors reach L + 1.
+constexpr int kGradMaxL = kMaxPairL;
+constexpr int kGradVec = 7;   // h, gA (x,y,z), gB (x,y,z)
+GCI_HD constexpr int grad_hb(int L) { return herm_n(L + 1); }   // entries of a bra vector / potential
+
+struct GradPotArgs {
+    const double* mP;        // per primitive pair: exponent sum P
+    const double* mX;        // product centre
+    const double* mY;
+    const double* mZ;
+    int64_t bra_beg, nbra;   // bra primitive pairs of level L1: global indices bra_beg ..
+    int64_t ket_beg, nket;   // ket primitive pairs of level L2
+    const double* hk;        // ket vectors of level L2, transposed: hk[tau * nket + k], sign (-1)^|tau| applied
+    double* V;               // potentials of level L1: V[i * grad_hb(L1) + t], accumulated atomically
+    int64_t chunk;           // ket primitive pairs per warp
+    int64_t nchunk;          // chunks per bra primitive pair
+    double kappa;
+    const double* boys;
+};
+
 } // namespace gci

@@ -36,4 +36,21 @@ cudaError_t launch_zero_upper(double* A, int64_t n, cudaStream_t s);
 cudaError_t launch_unpack_rkpq(const double* R, int64_t nvecs, const int64_t* pq_col, const int* pq_ao, int64_t npq,
                                int64_t k0, int64_t kc, int64_t nao, double* U, cudaStream_t s);
 
+// adjoint path (grad_kernels.cu)
+cudaError_t grad_module_init();
+cudaError_t grad_pair_vectors_launch(const ShellPairDev* pairs, int npairs, const int64_t* gbase,
+                                     const int* level_beg, const int* level_n, const int64_t* vec_off,
+                                     const int64_t* hk_off, const double* xyz, const int* poff, const double* exps,
+                                     const double* coefs, const int* plist, const double* tmat, const int* toff,
+                                     const int* nfunc, const int* loc, const double* D, int64_t ldd, double* mP,
+                                     double* mX, double* mY, double* mZ, double* vecs, double* hk, int* ppair,
+                                     cudaStream_t st);
+cudaError_t grad_potential_launch(int L1, int L2, const GradPotArgs& a, cudaStream_t st);
+cudaError_t grad_dots_launch(int64_t beg, int64_t n, int HB, const double* vecs, const double* V, double* out,
+                             cudaStream_t st);
+cudaError_t grad_coulomb_matrix_launch(const ShellPairDev* pairs, int npairs, const int64_t* gbase,
+                                       const int* level_beg, const int64_t* pot_off, const double* V, const double* pp,
+                                       const double* tmat, const int* toff, const int* nfunc, const int* loc,
+                                       double* J, int64_t ldj, cudaStream_t st);
+
 } // namespace gci

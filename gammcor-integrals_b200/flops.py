@@ -150,3 +150,25 @@ def kernel_flops(stats: np.ndarray, variants: dict, spher=True) -> float:
             prim, perb, perk, epi = kernel_class_flops(la, lb, lc, ld, variants.get((tb, tk), 0), spher)
             total += pq * prim + nbp * perb + nkp * perk + q * epi
     return total
+
+
+@lru_cache(maxsize=None)
+def grad_class_flops(L1, L2):
+    """Flops per primitive quartet of the adjoint potential kernel (grad_engine.cuh)
+    for a bra pair of Hermite level L1 and a ket pair of level L2: Boys values
+    and prefactor, the in-place R_tuv recursion to level N = L1 + 1 + L2, and
+    the contraction V(t) += sum_tau h(tau) R(t + tau) over t <= L1 + 1,
+    tau <= L2 (an FMA counted as two flops)."""
+    N = L1 + 1 + L2
+    boys = 30 + 3 * N
+    pref = 25
+    rrec = 3 * sum(herm_n(N - j) - 1 for j in range(N))
+    contraction = 2 * herm_n(L1 + 1) * herm_n(L2)
+    return boys + pref + rrec + contraction
+
+
+def grad_flops(work: np.ndarray) -> float:
+    """Total flops of one gci_coulomb_grad call from gci_coulomb_grad_work
+    (primitive quartets per (L1, L2), 7 x 7)."""
+    w = np.asarray(work).reshape(7, 7)
+    return float(sum(w[a, b] * grad_class_flops(a, b) for a in range(7) for b in range(7)))

@@ -178,6 +178,27 @@ int gci_eri_variant(int tb, int tk, int variant);
  * variant; 0 where not measured). */
 int gci_autotune_eri(const gci_basis *basis, int max_pairs, double *seconds);
 
+/* ---- adjoint: Coulomb energy and nuclear gradient (no counterpart in the reference) ---- */
+
+/* J = 1/2 sum_{pq,rs} D_pq (pq|rs) D_rs of a density D(ldd, NAO) (column-major, AO order of
+ * the basis; D is symmetrised) and its derivatives, from derivative integrals built by Hermite
+ * index shifts of the reference's McMurchie-Davidson scheme (E coefficients
+ * auto2e_Hermite.f90:10-423, R_tuv :425-11878, Boys boys.f90:224-281):
+ *   energy  J (may be NULL)
+ *   grad    dJ/dAtomCoords, 3 x NAtoms column-major (may be NULL)
+ *   jmat    Coulomb matrix J_pq = sum_rs (pq|rs) D_rs = dJ/dD_pq, ldj x NAO (may be NULL).
+ * omega <= 0: full-range Coulomb operator. */
+int gci_coulomb_grad(const gci_basis *basis, double omega, const double *D, int64_t ldd, double *energy,
+                     double *grad, double *jmat, int64_t ldj);
+
+/* gci_coulomb_grad with D and jmat in device memory (energy and grad stay host pointers). */
+int gci_coulomb_grad_device(const gci_basis *basis, double omega, const double *D_dev, int64_t ldd,
+                            double *energy, double *grad, double *jmat_dev, int64_t ldj);
+
+/* Primitive quartets evaluated by the last gci_coulomb_grad* call, per (bra level, ket level)
+ * of shell-pair Hermite levels lA+lB: out[L1 * 7 + L2], up to n entries (49). */
+int gci_coulomb_grad_work(double *out, int n);
+
 /* ---- allocation-free entry point (no counterpart in the reference) ---- */
 
 /* Size of the fixed device scratch behind gci_eri_pairs_noalloc: a file-scope
