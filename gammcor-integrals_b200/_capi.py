@@ -27,7 +27,7 @@ EXPORTS = ("gci_init", "gci_rkpq", "gci_query", "gci_copy_rkpq", "gci_copy_chol2
            "gci_rkab", "gci_timings", "gci_free", "gci_last_error", "gci_boys", "gci_spher_coeffs",
            "gci_normalize_basis", "gci_eri_pairs", "gci_rkab_device", "gci_stats", "gci_get_stream",
            "gci_kernel_launches", "gci_eri_pairs_noalloc", "gci_eri_variant", "gci_autotune_eri",
-           "gci_coulomb_grad", "gci_coulomb_grad_device", "gci_coulomb_grad_work")
+           "gci_coulomb_grad", "gci_coulomb_grad_device", "gci_coulomb_grad_work", "gci_rkpq_batch")
 
 _pd = C.POINTER(C.c_double)
 _pl = C.POINTER(C.c_int64)
@@ -59,6 +59,8 @@ def lib():
         L = C.CDLL(str(LIB_PATH))
         L.gci_init.argtypes = []
         L.gci_rkpq.argtypes = [C.POINTER(gci_basis), C.c_int, C.c_double, C.c_int, C.POINTER(C.c_void_p)]
+        L.gci_rkpq_batch.argtypes = [_i64, C.POINTER(gci_basis), C.c_int, C.c_double, C.c_int, C.c_int,
+                                     C.POINTER(C.c_void_p)]
         L.gci_query.argtypes = [C.c_void_p] + [_pl] * 6
         L.gci_copy_rkpq.argtypes = [C.c_void_p, _pd]
         L.gci_copy_chol2data.argtypes = [C.c_void_p] + [_pl] * 10 + [_pd]

@@ -95,7 +95,29 @@ def chol_gammcor_Rkpq(AOBasis: TAOBasis, Accuracy: int, Omega: float | None = No
             (_capi.GCI_FLAG_PIVOT_DECODE_STORAGE if decode_storage else 0)
     h = C.c_void_p()
     _capi.check(L.gci_rkpq(C.byref(b), int(Accuracy), float(Omega) if Omega else 0.0, flags, C.byref(h)))
-    handle = _Handle(h)
+    return _vecs_from_handle(_Handle(h), materialize and copy_to_host)
+
+
+def chol_gammcor_Rkpq_batch(AOBases, Accuracy: int, Omega: float | None = None, *, materialize: bool = True,
+                            copy_to_host: bool = True, nstreams: int = 16) -> list:
+    """chol_gammcor_Rkpq for many independent molecules in one call (gci_rkpq_batch): the
+    molecules run concurrently, one CUDA stream per worker.  Returns one TCholeskyVecsOTF per basis."""
+    L = _capi.lib()
+    n = len(AOBases)
+    views = [tb.c_struct() for tb in AOBases]   # each keeps its arrays alive; the array below copies pointers
+    structs = (_capi.gci_basis * n)(*views)
+    flags = _capi.GCI_FLAG_MATERIALIZE_RKPQ if materialize else 0
+    hs = (C.c_void_p * n)()
+    _capi.check(L.gci_rkpq_batch(n, structs, int(Accuracy), float(Omega) if Omega else 0.0, flags, int(nstreams),
+                                 hs))
+    out = [_vecs_from_handle(_Handle(C.c_void_p(hs[i])), materialize and copy_to_host) for i in range(n)]
+    del views
+    return out
+
+
+def _vecs_from_handle(handle: "_Handle", copy_rkpq: bool) -> TCholeskyVecsOTF:
+    L = _capi.lib()
+    h = handle.ptr
     dims = [C.c_int64() for _ in range(6)]
     _capi.check(L.gci_query(h, *[C.byref(d) for d in dims]))
     nvecs, msd, nsub, npq, nsp, npsp = (d.value for d in dims)
@@ -115,7 +137,7 @@ def chol_gammcor_Rkpq(AOBasis: TAOBasis, Accuracy: int, Omega: float | None = No
                        PivotShellPairs=psp, PivotShellPairLoc=pspl, PivotShellPairDim=pspd, PivotOrbPairs=porb,
                        NPivotShellPairs=npsp)
     rkpq = None
-    if materialize and copy_to_host:
+    if copy_rkpq:
         rkpq = np.zeros((nvecs, msd, nsub), order="F")
         _capi.check(L.gci_copy_rkpq(h, _capi.ptr(rkpq)))
     return TCholeskyVecsOTF(Rkpq=rkpq, Chol2Data=chol2, handle=handle, pivot_order=order, pivot_dmax=dm)

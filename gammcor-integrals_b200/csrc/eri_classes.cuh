@@ -20,11 +20,12 @@ static void launch_class(const EriArgs& args, cudaStream_t st)
     using G = EriTeam<LA, LB, LC, LD>;
     const size_t smem = G::smem_bytes();
     auto kern = k_eri_class<LA, LB, LC, LD>;
-    static bool attr_set = false;
-    if (!attr_set) {
+    // once per kernel, thread-safe (function-local static initialisation)
+    static const bool attr_set = [&] {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-    }
+        return true;
+    }();
+    (void)attr_set;
     const int64_t ntasks = (args.mode == kModeDiagonal) ? args.nbra : args.nbra * args.nket;
     if (ntasks <= 0) return;
     int64_t blocks = (ntasks + G::NT - 1) / G::NT;
@@ -46,11 +47,12 @@ static void launch_kf(const EriArgs& args, cudaStream_t st)
     using K = KfShape<LA, LB, LC, LD, TWQ>;
     const size_t smem = K::smem_bytes();
     auto kern = k_eri_kf<LA, LB, LC, LD, TWQ>;
-    static bool attr_set = false;
-    if (!attr_set) {
+    // once per kernel, thread-safe (function-local static initialisation)
+    static const bool attr_set = [&] {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-    }
+        return true;
+    }();
+    (void)attr_set;
     const int64_t ntasks = (args.mode == kModeDiagonal) ? args.nbra : args.nbra * args.nket;
     if (ntasks <= 0) return;
     int64_t blocks = (ntasks + K::TEAMS - 1) / K::TEAMS;

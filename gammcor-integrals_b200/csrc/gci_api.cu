@@ -20,6 +20,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace gci {
@@ -71,6 +72,12 @@ void count_launch(int64_t n) { g_launches += n; }
 int64_t launches() { return g_launches.load(); }
 
 // ------------------------------------------------------------------ device buffers
+// Stream of the calling thread's current context (set by ctx()).  Device
+// buffers are allocated and freed stream-ordered on it, so that a free does
+// not synchronise the whole device while other streams (the workers of a
+// batch) are running.
+static thread_local cudaStream_t t_stream = nullptr;
+
 template <class T>
 struct DVec {
     T* p = nullptr;
@@ -87,7 +94,7 @@ struct DVec {
     ~DVec() { release(); }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, t_stream);
         p = nullptr;
         n = 0;
     }
@@ -96,7 +103,7 @@ struct DVec {
         if (count == n && p) return;
         release();
         if (count == 0) return;
-        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+        cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), t_stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
             p = nullptr;
@@ -126,20 +133,35 @@ struct Context {
     DVec<int> err;
 };
 static Context g_ctx;
+// Worker contexts of gci_rkpq_batch (own stream, cuBLAS and cuSOLVER handles
+// and error word each; the Boys table is g_ctx's), kept for the process.
+static std::vector<std::unique_ptr<Context>> g_pool;
+// Context of a batch worker thread; nullptr: the process-wide g_ctx.
+static thread_local Context* t_cur = nullptr;
+
+static void context_streams(Context& c)
+{
+    CU(cudaGetDevice(&c.device));
+    CU(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    CB(cublasCreate(&c.blas));
+    CB(cublasSetStream(c.blas, c.stream));
+    CB(cublasSetMathMode(c.blas, CUBLAS_DEFAULT_MATH));
+    CS(cusolverDnCreate(&c.solver));
+    CS(cusolverDnSetStream(c.solver, c.stream));
+}
 
 static Context& ctx()
 {
+    if (t_cur) {
+        t_stream = t_cur->stream;
+        return *t_cur;
+    }
     if (!g_ctx.ready) {
         int ndev = 0;
         cudaError_t e = cudaGetDeviceCount(&ndev);
         if (e != cudaSuccess || ndev == 0) fail(GCI_ERR_CUDA, "no CUDA device available");
-        CU(cudaGetDevice(&g_ctx.device));
-        CU(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
-        CB(cublasCreate(&g_ctx.blas));
-        CB(cublasSetStream(g_ctx.blas, g_ctx.stream));
-        CB(cublasSetMathMode(g_ctx.blas, CUBLAS_DEFAULT_MATH));
-        CS(cusolverDnCreate(&g_ctx.solver));
-        CS(cusolverDnSetStream(g_ctx.solver, g_ctx.stream));
+        context_streams(g_ctx);
+        t_stream = g_ctx.stream;
         CU(eri_module_init());
         std::vector<double> tab = boys_table(kBoysMaxM);
         g_ctx.boys.upload(tab, g_ctx.stream);
@@ -148,7 +170,25 @@ static Context& ctx()
         CU(cudaStreamSynchronize(g_ctx.stream));
         g_ctx.ready = true;
     }
+    t_stream = g_ctx.stream;
     return g_ctx;
+}
+
+// The first n worker contexts, created on first use (calling thread, after g_ctx).
+static void ensure_pool(int n)
+{
+    Context& M = ctx();
+    while ((int)g_pool.size() < n) {
+        std::unique_ptr<Context> c(new Context());
+        context_streams(*c);
+        t_stream = c->stream;
+        c->err.alloc(1);
+        CU(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+        CU(cudaStreamSynchronize(c->stream));
+        c->ready = true;
+        g_pool.push_back(std::move(c));
+    }
+    t_stream = M.stream;
 }
 
 // ------------------------------------------------------------------ phase timer
@@ -482,7 +522,7 @@ static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<in
     a.nao = H.hb.nao;
     a.jcount = jcount;
     a.kappa = H.kappa;
-    a.boys = C.boys.p;
+    a.boys = g_ctx.boys.p;
     a.err = C.err.p;
     auto sums = [&](const std::vector<int>& g, int64_t lo, int64_t hi, double& np, double& nf, double& nu) {
         np = 0.0; nf = 0.0; nu = 0.0;
@@ -1108,6 +1148,7 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
     U.alloc((size_t)nao * nao * kc);
     W1.alloc((size_t)nao * NA * kc);
     PhaseTimer& T = H.timer;
+    T.s = s;   // this call's stream (the decomposition may have run on a batch worker's)
     if (H.have_rkpq) {
         // reference order: from the stored Rkpq (Cholesky_Gammcor.f90:143-332)
         std::vector<int64_t> pqcol;
@@ -1326,7 +1367,7 @@ static void coulomb_grad_impl(const gci_basis* basis, double omega, const double
             a.chunk = kChunk;
             a.nchunk = (ln[L2] + kChunk - 1) / kChunk;
             a.kappa = H.kappa;
-            a.boys = C.boys.p;
+            a.boys = g_ctx.boys.p;
             CU(grad_potential_launch(L1, L2, a, C.stream));
         }
     for (int L = 0; L < NL; ++L)
@@ -1364,6 +1405,24 @@ static void coulomb_grad_impl(const gci_basis* basis, double omega, const double
     if (grad) std::copy(g.begin(), g.end(), grad);
 }
 
+// chol_gammcor_Rkpq on the calling thread's context (stream).
+static void rkpq_run(Handle& H, const gci_basis* basis, int accuracy, double omega, int flags)
+{
+    H.tau = accuracy_tau(accuracy);
+    H.kappa = (omega > 0.0) ? 1.0 / (omega * omega) : 0.0;   // Cholesky_Gammcor.f90:412-421
+    H.flags = flags;
+    Context& C = ctx();
+    H.timer.s = C.stream;
+    auto t0 = std::chrono::steady_clock::now();
+    H.hb = make_basis(basis);
+    setup_pairs(H);
+    step1(H);
+    step2(H);
+    if (flags & GCI_FLAG_MATERIALIZE_RKPQ) materialize_rkpq(H);
+    CU(cudaStreamSynchronize(C.stream));
+    H.t_rkpq = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
 extern "C" {
 
 int gci_init(void)
@@ -1376,24 +1435,68 @@ int gci_rkpq(const gci_basis* basis, int accuracy, double omega, int flags, gci_
     if (!out) { g_last_error = "out is NULL"; return GCI_ERR_ARG; }
     *out = nullptr;
     std::unique_ptr<gci_handle> hp(new gci_handle());
-    const int rc = guarded([&] {
-        Handle& H = hp->h;
-        H.tau = accuracy_tau(accuracy);
-        H.kappa = (omega > 0.0) ? 1.0 / (omega * omega) : 0.0;   // Cholesky_Gammcor.f90:412-421
-        H.flags = flags;
-        Context& C = ctx();
-        H.timer.s = C.stream;
-        auto t0 = std::chrono::steady_clock::now();
-        H.hb = make_basis(basis);
-        setup_pairs(H);
-        step1(H);
-        step2(H);
-        if (flags & GCI_FLAG_MATERIALIZE_RKPQ) materialize_rkpq(H);
-        CU(cudaStreamSynchronize(C.stream));
-        H.t_rkpq = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    });
+    const int rc = guarded([&] { rkpq_run(hp->h, basis, accuracy, omega, flags); });
     if (rc == GCI_OK) *out = hp.release();
     return rc;
+}
+
+int gci_rkpq_batch(int64_t nmol, const gci_basis* bases, int accuracy, double omega, int flags, int nstreams,
+                   gci_handle** out)
+{
+    if (!bases || !out || nmol < 0) { g_last_error = "invalid argument"; return GCI_ERR_ARG; }
+    for (int64_t i = 0; i < nmol; ++i) out[i] = nullptr;
+    if (nmol == 0) return GCI_OK;
+    int nw = nstreams > 0 ? nstreams : 16;
+    nw = (int)std::min<int64_t>(std::min(nw, 64), nmol);
+    const int rc0 = guarded([&] { ensure_pool(nw); });
+    if (rc0 != GCI_OK) return rc0;
+    // largest molecules first (work estimate: shells^2), taken from one queue
+    std::vector<int64_t> order(nmol);
+    for (int64_t i = 0; i < nmol; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t a, int64_t b) { return bases[a].nshells > bases[b].nshells; });
+    std::vector<std::unique_ptr<gci_handle>> hs(nmol);
+    std::atomic<int64_t> next{0};
+    std::atomic<bool> stop{false};
+    std::mutex em;
+    int err_code = GCI_OK;
+    int64_t err_mol = -1;
+    std::string err_msg;
+    auto worker = [&](int w) {
+        t_cur = g_pool[w].get();
+        for (;;) {
+            if (stop.load()) break;
+            const int64_t q = next.fetch_add(1);
+            if (q >= nmol) break;
+            const int64_t i = order[q];
+            std::unique_ptr<gci_handle> hp(new gci_handle());
+            const int rc = guarded([&] { rkpq_run(hp->h, &bases[i], accuracy, omega, flags); });
+            if (rc != GCI_OK) {
+                std::lock_guard<std::mutex> lock(em);
+                if (err_code == GCI_OK || i < err_mol) {
+                    err_code = rc;
+                    err_mol = i;
+                    err_msg = g_last_error;
+                }
+                stop.store(true);
+                break;
+            }
+            hs[i] = std::move(hp);
+        }
+        t_cur = nullptr;
+    };
+    std::vector<std::thread> th;
+    for (int w = 1; w < nw; ++w) th.emplace_back(worker, w);
+    worker(0);
+    for (auto& t : th) t.join();
+    t_stream = g_ctx.stream;
+    if (err_code != GCI_OK) {
+        hs.clear();
+        g_last_error = "molecule " + std::to_string(err_mol) + ": " + err_msg;
+        return err_code;
+    }
+    for (int64_t i = 0; i < nmol; ++i) out[i] = hs[i].release();
+    return GCI_OK;
 }
 
 int gci_query(const gci_handle* h, int64_t* nvecs, int64_t* max_subset_dim, int64_t* nsubsets, int64_t* norbpairs,
@@ -1544,7 +1647,7 @@ int gci_boys(int m, int64_t n, const double* x, double* out)
         std::vector<double> hx(x, x + n);
         dx.upload(hx, C.stream);
         dout.alloc((size_t)std::max<int64_t>(n, 1) * (m + 1));
-        CU(boys_eval_launch(m, n, dx.p, C.boys.p, dout.p, C.stream));
+        CU(boys_eval_launch(m, n, dx.p, g_ctx.boys.p, dout.p, C.stream));
         if (n) CU(cudaMemcpyAsync(out, dout.p, sizeof(double) * n * (m + 1), cudaMemcpyDeviceToHost, C.stream));
         CU(cudaStreamSynchronize(C.stream));
     });

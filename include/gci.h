@@ -83,6 +83,16 @@ int gci_init(void);
  * the full-range Coulomb operator (Kappa = 0). */
 int gci_rkpq(const gci_basis *basis, int accuracy, double omega, int flags, gci_handle **out);
 
+/* gci_rkpq for many independent molecules at once (the reference decomposes one molecule per
+ * chol_gammcor_Rkpq call, Cholesky_Gammcor.f90:335-377).  The molecules are taken largest
+ * first from one queue by nstreams host workers (<= 0: 16; at most 64), each with its own
+ * CUDA stream and cuBLAS/cuSOLVER handles, so that the kernels of different molecules run
+ * concurrently on the GPU.  out[i] receives the handle of bases[i] (same results as gci_rkpq
+ * on that basis).  On an error no handle is returned (all out[i] = NULL) and
+ * gci_last_error() names the lowest-index molecule that failed. */
+int gci_rkpq_batch(int64_t nmol, const gci_basis *bases, int accuracy, double omega, int flags, int nstreams,
+                   gci_handle **out);
+
 /* Dimensions of TCholeskyVecsOTF / TChol2Vecs (TwoStepCholesky_definitions.f90:56-74). */
 int gci_query(const gci_handle *h, int64_t *nvecs, int64_t *max_subset_dim, int64_t *nsubsets,
               int64_t *norbpairs, int64_t *nshellpairs, int64_t *npivshellpairs);
