@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--buffer-mb", type=int, default=16384)
     ap.add_argument("--tune-pairs", type=int, default=40, help="shell pairs per class sampled by the ERI autotuner")
+    ap.add_argument("--streams", type=int, default=32, help="c3: workers (CUDA streams) of gci_rkpq_batch")
     ap.add_argument("--decode-storage", action="store_true",
                     help="decode diagonal-shell-pair pivots in storage order (GCI_FLAG_PIVOT_DECODE_STORAGE)")
     return ap.parse_args()
@@ -302,7 +303,7 @@ def run_batch(args, local):
     tune = np.zeros(400)
     _capi.check(L.gci_autotune_eri(C.byref(views[int(np.argmax([tb.NAO for tb in tbs]))]), args.tune_pairs,
                                    _capi.ptr(tune)))
-    nstreams = 32
+    nstreams = args.streams
 
     def batch():
         hs = (C.c_void_p * 64)()

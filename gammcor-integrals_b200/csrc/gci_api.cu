@@ -77,6 +77,11 @@ int64_t launches() { return g_launches.load(); }
 // not synchronise the whole device while other streams (the workers of a
 // batch) are running.
 static thread_local cudaStream_t t_stream = nullptr;
+// The library's own memory pool: freed blocks up to kPoolKeepBytes stay mapped
+// for the next allocation (mapping device memory costs more than the kernels
+// of a small molecule); the pool is created with the process-wide context.
+static cudaMemPool_t g_mempool = nullptr;
+constexpr uint64_t kPoolKeepBytes = (uint64_t)8 << 30;
 
 template <class T>
 struct DVec {
@@ -103,7 +108,8 @@ struct DVec {
         if (count == n && p) return;
         release();
         if (count == 0) return;
-        cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), t_stream);
+        cudaError_t e = g_mempool ? cudaMallocFromPoolAsync((void**)&p, count * sizeof(T), g_mempool, t_stream)
+                                  : cudaMallocAsync((void**)&p, count * sizeof(T), t_stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
             p = nullptr;
@@ -162,6 +168,16 @@ static Context& ctx()
         if (e != cudaSuccess || ndev == 0) fail(GCI_ERR_CUDA, "no CUDA device available");
         context_streams(g_ctx);
         t_stream = g_ctx.stream;
+        if (!g_mempool) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = g_ctx.device;
+            CU(cudaMemPoolCreate(&g_mempool, &props));
+            uint64_t keep = kPoolKeepBytes;
+            CU(cudaMemPoolSetAttribute(g_mempool, cudaMemPoolAttrReleaseThreshold, &keep));
+        }
         CU(eri_module_init());
         std::vector<double> tab = boys_table(kBoysMaxM);
         g_ctx.boys.upload(tab, g_ctx.stream);
