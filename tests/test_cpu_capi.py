@@ -52,3 +52,37 @@ def test_noalloc_rejects_oversized_basis_before_device_work():
     assert rc == _capi.GCI_ERR_BUFFER
     msg = _capi.lib().gci_last_error().decode()
     assert "scratch" in msg and str(_capi.GCI_NOALLOC_SCRATCH_BYTES) in msg
+
+
+def test_coulomb_grad_and_batch_argument_errors_without_device_work():
+    """Argument checks of the adjoint and batch entry points come before any
+    CUDA call (no GPU needed): a NULL density, nothing requested, and an empty
+    batch."""
+    import ctypes as C
+    mol = molecules.small_molecule(3, natoms=2, recipe=(0, 1))
+    tb = gbasis.from_molecule(mol)
+    s = tb.c_struct()
+    L = _capi.lib()
+    e = C.c_double()
+    g = np.zeros(3 * tb.NAtoms)
+    assert L.gci_coulomb_grad(C.byref(s), 0.0, None, tb.NAO, C.byref(e), _capi.ptr(g), None, tb.NAO) == -1
+    assert b"D is NULL" in L.gci_last_error()
+    D = np.eye(tb.NAO)
+    assert L.gci_coulomb_grad(C.byref(s), 0.0, _capi.ptr(D), tb.NAO, None, None, None, tb.NAO) == -1
+    assert b"nothing requested" in L.gci_last_error()
+    hs = (C.c_void_p * 1)()
+    arr = (_capi.gci_basis * 1)(s)
+    assert L.gci_rkpq_batch(0, arr, 1, 0.0, 0, 4, hs) == 0
+    assert L.gci_rkpq_batch(-1, arr, 1, 0.0, 0, 4, hs) == -1
+
+
+def test_adjoint_work_model():
+    """flops.grad_class_flops counts the potential kernel's arithmetic: the
+    contraction H(L1+1) H(L2) FMAs dominates, the recursion grows with N."""
+    from gammcor_integrals_b200 import flops
+    f = flops.grad_class_flops
+    assert f(0, 0) == 30 + 3 * 1 + 25 + 3 * (flops.herm_n(1) - 1) + 2 * 4 * 1
+    assert f(4, 4) > f(4, 3) > f(3, 3)
+    w = np.zeros(49)
+    w[2 * 7 + 1] = 10.0
+    assert flops.grad_flops(w) == 10.0 * f(2, 1)
