@@ -59,7 +59,7 @@ struct KfShape {
     static constexpr int NCH = (S::NF + CH - 1) / CH;
     // ket primitive pairs whose Boys values and geometry are prepared at once
     // (one per lane) and the stride of their entries: F_0..F_LT, X, Y, Z
-    static constexpr int KB = 32, FS = S::LT + 4;
+    static constexpr int KB = 16, FS = S::LT + 4;
     // team scratch (doubles): R ping-pong, V and the prepared ket primitives
     // during the primitive loop; the epilogue's two buffers of NE*NF
     // afterwards (W in registers) or W kept apart from them (W in shared memory)
@@ -68,9 +68,14 @@ struct KfShape {
     static constexpr int O_W = WREG ? 0 : cmax(SZ_LOOP, S::NE * S::NF);
     static constexpr int SZ = WREG ? cmax(SZ_LOOP, 2 * S::NE * S::NF) : O_W + S::NE * S::NF;
     // per-block tables: R recursion recipe of every Hermite index (its
-    // coefficient as a double, then ints: source indices and axis); R index
-    // of h + g; Hermite index of every bra product; first bra product of each ab
-    static constexpr int TAB_INTS = S::HT + S::H2 * S::H1 + S::NCB + S::NE + 1;
+    // coefficient as a double, then an int: source indices and axis); then
+    // 16-bit entries (every value is below 2^15): R index of h + g, Hermite
+    // index of every bra product, first bra product of each ab.  The 16-bit
+    // tables and 16 prepared ket primitives keep the (f,f|f,d) block within
+    // half of an SM's shared memory (two blocks per SM)
+    static constexpr int TAB_INTS = S::HT;
+    static constexpr int TAB_SHORTS = S::H2 * S::H1 + S::NCB + S::NE + 1;
+    static_assert(S::HT < 32768 && S::NCB < 32768, "16-bit tables");
     // teams per block: four warps while their scratch stays within 160 KB
     static constexpr int TEAMS = TW > 32 ? 1
                                          : ((size_t)SZ * 8 * 4 <= 160 * 1024 ? 4
@@ -78,7 +83,8 @@ struct KfShape {
     static constexpr int TPB = TW > 32 ? TW : 32 * TEAMS;
     static constexpr size_t smem_bytes()
     {
-        return sizeof(double) * ((size_t)TEAMS * SZ + S::HT) + sizeof(int) * (size_t)TAB_INTS;
+        return sizeof(double) * ((size_t)TEAMS * SZ + S::HT) + sizeof(int) * (size_t)TAB_INTS +
+               sizeof(short) * (size_t)TAB_SHORTS;
     }
 };
 
@@ -92,9 +98,9 @@ k_eri_kf(const EriArgs a)
     extern __shared__ double smem[];
     double* tab_coef = smem + (size_t)K::TEAMS * K::SZ;           // recursion coefficient of h
     int* tab_rec = reinterpret_cast<int*>(tab_coef + S::HT);       // i1 | i2 << 12 | axis << 24
-    int* tab_ridx = tab_rec + S::HT;             // [g][h] -> herm_idx(h + g)
-    int* tab_cbh = tab_ridx + S::H2 * S::H1;     // bra product -> Hermite index
-    int* tab_cbo = tab_cbh + S::NCB;             // ab -> first bra product
+    short* tab_ridx = reinterpret_cast<short*>(tab_rec + S::HT);   // [g][h] -> herm_idx(h + g)
+    short* tab_cbh = tab_ridx + S::H2 * S::H1;   // bra product -> Hermite index
+    short* tab_cbo = tab_cbh + S::NCB;           // ab -> first bra product
 
     // R^{(j)}_{tuv} = d R^{(j+1)}_{tuv - e} + (n - 1) R^{(j+1)}_{tuv - 2e} along the first
     // nonzero axis e of (t,u,v) with component n (d = X, Y or Z); h = 0 takes F_j
@@ -109,18 +115,18 @@ k_eri_kf(const EriArgs a)
     }
     for (int c = threadIdx.x; c < S::H2 * S::H1; c += TPB) {
         const int g = c / S::H1, h = c - g * S::H1;
-        tab_ridx[c] = herm_idx(herm_t(h) + herm_t(g), herm_u(h) + herm_u(g), herm_v(h) + herm_v(g));
+        tab_ridx[c] = (short)herm_idx(herm_t(h) + herm_t(g), herm_u(h) + herm_u(g), herm_v(h) + herm_v(g));
     }
     for (int e = threadIdx.x; e < S::NE; e += TPB) {
         int off = 0;
         for (int f = 0; f < e; ++f) off += pair_supp(LA, LB, f);
-        tab_cbo[e] = off;
+        tab_cbo[e] = (short)off;
         const int ex = pair_x(LA, LB, e), ey = pair_y(LA, LB, e), ez = pair_z(LA, LB, e);
         for (int v = 0; v <= ez; ++v)
             for (int u = 0; u <= ey; ++u)
-                for (int t = 0; t <= ex; ++t) tab_cbh[off++] = herm_idx(t, u, v);
+                for (int t = 0; t <= ex; ++t) tab_cbh[off++] = (short)herm_idx(t, u, v);
     }
-    if (threadIdx.x == 0) tab_cbo[S::NE] = S::NCB;
+    if (threadIdx.x == 0) tab_cbo[S::NE] = (short)S::NCB;
     __syncthreads();
 
     const int team = threadIdx.x / TW;

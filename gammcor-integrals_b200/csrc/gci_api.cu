@@ -77,11 +77,18 @@ int64_t launches() { return g_launches.load(); }
 // not synchronise the whole device while other streams (the workers of a
 // batch) are running.
 static thread_local cudaStream_t t_stream = nullptr;
-// The library's own memory pool: freed blocks up to kPoolKeepBytes stay mapped
-// for the next allocation (mapping device memory costs more than the kernels
-// of a small molecule); the pool is created with the process-wide context.
+// The library's own memory pool.  Freed blocks stay mapped for the rest of a
+// call (mapping device memory costs more than the kernels of a small molecule,
+// and re-mapping the multi-GB Cholesky buffers inside the stream would stall
+// it); when a top-level call returns, the pool is trimmed to kPoolKeepBytes.
+// The pool is created with the process-wide context.
 static cudaMemPool_t g_mempool = nullptr;
 constexpr uint64_t kPoolKeepBytes = (uint64_t)8 << 30;
+
+static void pool_trim()
+{
+    if (g_mempool) cudaMemPoolTrimTo(g_mempool, (size_t)kPoolKeepBytes);
+}
 
 template <class T>
 struct DVec {
@@ -175,7 +182,7 @@ static Context& ctx()
             props.location.type = cudaMemLocationTypeDevice;
             props.location.id = g_ctx.device;
             CU(cudaMemPoolCreate(&g_mempool, &props));
-            uint64_t keep = kPoolKeepBytes;
+            uint64_t keep = ~(uint64_t)0;   // no release at synchronisation; pool_trim() after each call
             CU(cudaMemPoolSetAttribute(g_mempool, cudaMemPoolAttrReleaseThreshold, &keep));
         }
         CU(eri_module_init());
@@ -1453,6 +1460,8 @@ int gci_rkpq(const gci_basis* basis, int accuracy, double omega, int flags, gci_
     std::unique_ptr<gci_handle> hp(new gci_handle());
     const int rc = guarded([&] { rkpq_run(hp->h, basis, accuracy, omega, flags); });
     if (rc == GCI_OK) *out = hp.release();
+    else hp.reset();
+    pool_trim();
     return rc;
 }
 
@@ -1508,10 +1517,12 @@ int gci_rkpq_batch(int64_t nmol, const gci_basis* bases, int accuracy, double om
     t_stream = g_ctx.stream;
     if (err_code != GCI_OK) {
         hs.clear();
+        pool_trim();
         g_last_error = "molecule " + std::to_string(err_mol) + ": " + err_msg;
         return err_code;
     }
     for (int64_t i = 0; i < nmol; ++i) out[i] = hs[i].release();
+    pool_trim();
     return GCI_OK;
 }
 
@@ -1589,22 +1600,26 @@ int gci_rkab(gci_handle* h, const double* CA, int64_t ldca, int64_t a0, int64_t 
              int64_t ldcb, int64_t b0, int64_t b1, int64_t max_buffer_mb, int precision, double* rkab)
 {
     if (!h || !CA || !CB || !rkab) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
-    return guarded([&] {
+    const int rc = guarded([&] {
         auto t0 = std::chrono::steady_clock::now();
         rkab_impl(h->h, CA, ldca, a0, a1, CB, ldcb, b0, b1, max_buffer_mb, precision, rkab, false);
         h->h.t_rkab = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     });
+    pool_trim();
+    return rc;
 }
 
 int gci_rkab_device(gci_handle* h, const double* CA, int64_t ldca, int64_t a0, int64_t a1, const double* CB,
                     int64_t ldcb, int64_t b0, int64_t b1, int64_t max_buffer_mb, int precision, double* rkab)
 {
     if (!h || !CA || !CB || !rkab) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
-    return guarded([&] {
+    const int rc = guarded([&] {
         auto t0 = std::chrono::steady_clock::now();
         rkab_impl(h->h, CA, ldca, a0, a1, CB, ldcb, b0, b1, max_buffer_mb, precision, rkab, true);
         h->h.t_rkab = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     });
+    pool_trim();
+    return rc;
 }
 
 int gci_stats(const gci_handle* h, double* out, int n)
@@ -1650,7 +1665,11 @@ int gci_timings(const gci_handle* h, double* out, int n)
     return GCI_OK;
 }
 
-void gci_free(gci_handle* h) { delete h; }
+void gci_free(gci_handle* h)
+{
+    delete h;
+    pool_trim();
+}
 
 const char* gci_last_error(void) { return g_last_error.c_str(); }
 
@@ -1931,13 +1950,17 @@ int gci_eri_pairs_noalloc(const gci_basis* basis, double omega, double* out_dev,
 int gci_coulomb_grad(const gci_basis* basis, double omega, const double* D, int64_t ldd, double* energy,
                      double* grad, double* jmat, int64_t ldj)
 {
-    return guarded([&] { coulomb_grad_impl(basis, omega, D, ldd, false, energy, grad, jmat, ldj); });
+    const int rc = guarded([&] { coulomb_grad_impl(basis, omega, D, ldd, false, energy, grad, jmat, ldj); });
+    pool_trim();
+    return rc;
 }
 
 int gci_coulomb_grad_device(const gci_basis* basis, double omega, const double* D_dev, int64_t ldd, double* energy,
                             double* grad, double* jmat_dev, int64_t ldj)
 {
-    return guarded([&] { coulomb_grad_impl(basis, omega, D_dev, ldd, true, energy, grad, jmat_dev, ldj); });
+    const int rc = guarded([&] { coulomb_grad_impl(basis, omega, D_dev, ldd, true, energy, grad, jmat_dev, ldj); });
+    pool_trim();
+    return rc;
 }
 
 int gci_coulomb_grad_work(double* out, int n)
