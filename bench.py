@@ -108,6 +108,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(seconds: float, world: int, device) -> float:
+    """The slowest rank's time: every rank takes part in the same all-reduce
+    (MAX) whenever more than one rank runs."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(work_per_step: float, steps: int, world: int, t_max: float) -> float:
+    """Whole-job rate of independent replicas: the work of all ranks over the slowest rank's time."""
+    return work_per_step * steps * world / t_max
+
+
 def measured_fp64_peak(torch):
     """FP64 reference rate for the roofline (MEASURED_PEAKS.json has no FP64
     figure): cuBLAS DGEMM 8192^3, best of 5, CUDA events."""
@@ -153,6 +169,8 @@ def run_reference(args, rank):
     """--impl reference: the oracle on a bounded sample of the same workload."""
     if rank != 0:
         return
+    import gammcor_pkg
+    gammcor_pkg.load()
     from gammcor_integrals_b200 import flops, molecules
     from oracle import oracle as O
     m = molecules.config(args.config)
@@ -469,13 +487,10 @@ def main():
     del flush
     n1 = C.c_int64()
     _capi.check(L.gci_kernel_launches(C.byref(n1)))
-    t_tensor = torch.tensor([t_dev], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t_tensor, op=dist.ReduceOp.MAX)
-    t_max = float(t_tensor.item())
+    t_max = max_over_ranks(t_dev, world, "cuda")
     fl = flops.job_flops(stats[-1], "lib")
     flops_step = fl["total"]
-    value = flops_step * args.steps * world / t_max / 1e9
+    value = aggregate_rate(flops_step, args.steps, world, t_max) / 1e9
 
     # ---- end to end through the public host API (pinned host buffers)
     e2e = None
@@ -495,13 +510,10 @@ def main():
             del res
         e1.record(lib_stream)
         e1.synchronize()
-        te = torch.tensor([e0.elapsed_time(e1) * 1e-3], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        te = float(te.item())
+        te = max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, "cuda")
         h2d = int(Cm.nbytes) + int(tb.CntrCoeffs.nbytes + tb.Exponents.nbytes + tb.AtomCoords.nbytes)
         d2h = nv * NA * NB * 8
-        e2e = {"value": flops_step * args.e2e_steps * world / te / 1e9, "unit": "GFLOP/s",
+        e2e = {"value": aggregate_rate(flops_step, args.e2e_steps, world, te) / 1e9, "unit": "GFLOP/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "seconds_per_step": te / args.e2e_steps,
                "checksum": checksum}
 
