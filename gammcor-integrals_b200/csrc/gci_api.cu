@@ -1148,6 +1148,8 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
     if (NA <= 0 || NB <= 0) fail(GCI_ERR_ARG, "Invalid dimension of Rkab");
     if (ldca < nao || ldcb < nao) fail(GCI_ERR_ARG, "Invalid number of atomic orbitals in CA/CB");
     if (precision != GCI_PREC_FP64 && precision != GCI_PREC_MIXED) fail(GCI_ERR_ARG, "invalid precision mode");
+    if (precision == GCI_PREC_MIXED)
+        fail(GCI_ERR_UNSUPPORTED, "split-precision AO->MO GEMMs are not built (use GCI_PREC_FP64)");
     if (N == 0) return;
     // MO coefficient blocks on the device
     DVec<double> dCA, dCB, dOut, U, W1;
@@ -1431,6 +1433,8 @@ static void coulomb_grad_impl(const gci_basis* basis, double omega, const double
 // chol_gammcor_Rkpq on the calling thread's context (stream).
 static void rkpq_run(Handle& H, const gci_basis* basis, int accuracy, double omega, int flags)
 {
+    if (flags & GCI_FLAG_MIXED_STEP1)
+        fail(GCI_ERR_UNSUPPORTED, "split-precision GEMMs for the pivot search are not built (FP64 only)");
     H.tau = accuracy_tau(accuracy);
     H.kappa = (omega > 0.0) ? 1.0 / (omega * omega) : 0.0;   // Cholesky_Gammcor.f90:412-421
     H.flags = flags;

@@ -25,7 +25,7 @@ extern "C" {
 #define GCI_OK                 0
 #define GCI_ERR_ARG           -1   /* invalid argument / dimension       */
 #define GCI_ERR_CUDA          -2   /* CUDA, cuBLAS or cuSOLVER failure    */
-#define GCI_ERR_UNSUPPORTED   -3   /* angular momentum beyond the kernels */
+#define GCI_ERR_UNSUPPORTED   -3   /* angular momentum beyond the kernels, or a mode not built */
 #define GCI_ERR_NOT_CONVERGED -4   /* MaxNCholesky reached unconverged    */
 #define GCI_ERR_NOT_SPD       -5   /* pivot block V_JJ not positive definite */
 #define GCI_ERR_BUFFER        -6   /* buffer too small                    */
@@ -42,9 +42,10 @@ extern "C" {
 #define GCI_FLAG_MATERIALIZE_RKPQ   1  /* store Rkpq on the device (otherwise Rkab is built from V(pq,J) directly) */
 #define GCI_FLAG_PIVOT_DECODE_STORAGE 2 /* decode diagonal-shell-pair pivots in storage order (the reference decodes
                                           them with chol2_pq2p_ge_q, TwoStepCholesky_Step2.f90:422-466) */
-#define GCI_FLAG_MIXED_STEP1        4  /* split-precision tensor-core GEMMs in the pivot search */
+#define GCI_FLAG_MIXED_STEP1        4  /* split-precision GEMMs in the pivot search: not built, rejected with
+                                          GCI_ERR_UNSUPPORTED */
 
-/* Precision of the AO->MO GEMMs */
+/* Precision of the AO->MO GEMMs (GCI_PREC_MIXED, split precision, is not built: GCI_ERR_UNSUPPORTED) */
 #define GCI_PREC_FP64   0
 #define GCI_PREC_MIXED  1
 

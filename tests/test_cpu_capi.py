@@ -86,3 +86,15 @@ def test_adjoint_work_model():
     w = np.zeros(49)
     w[2 * 7 + 1] = 10.0
     assert flops.grad_flops(w) == 10.0 * f(2, 1)
+
+
+def test_split_precision_step1_flag_is_rejected_not_ignored():
+    """GCI_FLAG_MIXED_STEP1 names a mode that is not built: gci_rkpq refuses it
+    (GCI_ERR_UNSUPPORTED) before any device work instead of running FP64."""
+    import ctypes as C
+    mol = molecules.small_molecule(3, natoms=2, recipe=(0, 1))
+    s = gbasis.from_molecule(mol).c_struct()
+    h = C.c_void_p()
+    rc = _capi.lib().gci_rkpq(C.byref(s), 2, 0.0, _capi.GCI_FLAG_MIXED_STEP1, C.byref(h))
+    assert rc == -3 and not h.value
+    assert b"not built" in _capi.lib().gci_last_error()
