@@ -1475,6 +1475,9 @@ int gci_rkpq_batch(int64_t nmol, const gci_basis* bases, int accuracy, double om
     if (!bases || !out || nmol < 0) { g_last_error = "invalid argument"; return GCI_ERR_ARG; }
     for (int64_t i = 0; i < nmol; ++i) out[i] = nullptr;
     if (nmol == 0) return GCI_OK;
+    // the worker contexts are shared: batches from different caller threads run one after another
+    static std::mutex batch_mutex;
+    std::lock_guard<std::mutex> batch_lock(batch_mutex);
     int nw = nstreams > 0 ? nstreams : 16;
     nw = (int)std::min<int64_t>(std::min(nw, 64), nmol);
     const int rc0 = guarded([&] { ensure_pool(nw); });

@@ -90,7 +90,8 @@ int gci_rkpq(const gci_basis *basis, int accuracy, double omega, int flags, gci_
  * CUDA stream and cuBLAS/cuSOLVER handles, so that the kernels of different molecules run
  * concurrently on the GPU.  out[i] receives the handle of bases[i] (same results as gci_rkpq
  * on that basis).  On an error no handle is returned (all out[i] = NULL) and
- * gci_last_error() names the lowest-index molecule that failed. */
+ * gci_last_error() names the lowest-index molecule that failed.  Batch calls from
+ * different caller threads run one after another. */
 int gci_rkpq_batch(int64_t nmol, const gci_basis *bases, int accuracy, double omega, int flags, int nstreams,
                    gci_handle **out);
 
