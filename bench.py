@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--buffer-mb", type=int, default=16384)
     ap.add_argument("--tune-pairs", type=int, default=40, help="shell pairs per class sampled by the ERI autotuner")
+    ap.add_argument("--eri-kernels", default="hermite", choices=["hermite", "class"],
+                    help="product stages on the Hermite-matrix tensor-core kernels or the per-class kernels")
+    ap.add_argument("--hm-profile", action="store_true",
+                    help="diagnostic: time every Hermite-matrix class launch (serialised) and print the table")
     ap.add_argument("--streams", type=int, default=32, help="c3: workers (CUDA streams) of gci_rkpq_batch")
     ap.add_argument("--decode-storage", action="store_true",
                     help="decode diagonal-shell-pair pivots in storage order (GCI_FLAG_PIVOT_DECODE_STORAGE)")
@@ -221,6 +225,7 @@ def run_grad(args, rank, world, local):
     gammcor_pkg.load()
     from gammcor_integrals_b200 import _capi, basis, flops, molecules
     L = _capi.lib()
+    L.gci_eri_hm(1 if args.eri_kernels == "hermite" else 0)
     _capi.check(L.gci_init())
     mol = molecules.config("c4")
     tb = basis.from_molecule(mol)
@@ -313,6 +318,7 @@ def run_batch(args, local):
     gammcor_pkg.load()
     from gammcor_integrals_b200 import _capi, basis, flops, molecules
     L = _capi.lib()
+    L.gci_eri_hm(1 if args.eri_kernels == "hermite" else 0)
     _capi.check(L.gci_init())
     mols = [molecules.config("c3", i) for i in range(64)]
     tbs = [basis.from_molecule(m) for m in mols]
@@ -413,6 +419,7 @@ def main():
     from gammcor_integrals_b200 import _capi, basis, flops, molecules
     from gammcor_integrals_b200 import cholesky_gammcor as cg
     L = _capi.lib()
+    L.gci_eri_hm((2 if args.hm_profile else 1) if args.eri_kernels == "hermite" else 0)
     _capi.check(L.gci_init())
 
     def barrier():
@@ -453,10 +460,13 @@ def main():
             state["nvecs"] = nv.value
         _capi.check(L.gci_rkab_device(h, C.c_void_p(c_dev.data_ptr()), nao, a0, a1, C.c_void_p(c_dev.data_ptr()),
                                       nao, b0, b1, args.buffer_mb, prec, C.c_void_p(state["rkab"].data_ptr())))
-        st = np.zeros(8 + 600)
+        st = np.zeros(8 + 600 + 1)
         _capi.check(L.gci_stats(h, _capi.ptr(st), st.size))
         tm = np.zeros(13)
         _capi.check(L.gci_timings(h, _capi.ptr(tm), 13))
+        hs = np.zeros(7 * 7 * 3 * 3)
+        _capi.check(L.gci_eri_hm_stats(h, _capi.ptr(hs), hs.size))
+        state["hm"] = hs.reshape(7, 7, 3, 3)
         L.gci_free(h)
         return st, tm
 
@@ -488,6 +498,15 @@ def main():
     n1 = C.c_int64()
     _capi.check(L.gci_kernel_launches(C.byref(n1)))
     t_max = max_over_ranks(t_dev, world, "cuda")
+    if args.hm_profile and rank == 0:
+        hs = state["hm"]
+        tot = hs[..., 1].sum()
+        rows = sorted(((hs[a, b, c, 1], a, b, c + 1, hs[a, b, c, 0], hs[a, b, c, 2])
+                       for a in range(7) for b in range(7) for c in range(3) if hs[a, b, c, 0] > 0), reverse=True)
+        print(f"# Hermite-matrix classes: {tot:.2f} s, {hs[..., 2].sum() / 1e12:.1f} TFLOP issued", file=sys.stderr)
+        for t, a, b, c, n, f in rows:
+            print(f"#  L1={a} L2={b} NT={c}  launches {int(n):5d}  {t:8.3f} s  {100 * t / max(tot, 1e-30):5.1f}%  "
+                  f"{f / 1e12:8.2f} TF  {f / max(t, 1e-30) / 1e12:6.2f} TF/s", file=sys.stderr)
     fl = flops.job_flops(stats[-1], "lib")
     flops_step = fl["total"]
     value = aggregate_rate(flops_step, args.steps, world, t_max) / 1e9
@@ -534,7 +553,8 @@ def main():
             "achieved": eri_rate, "peak": peak64,
             "unit": "TFLOP/s", "frac": eri_rate / peak64 if peak64 else None, "traffic": None,
             "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64; MEASURED_PEAKS.json has no FP64 figure)",
-            "eri_seconds": eri_t, "gemm_seconds": gemm_t}
+            "eri_seconds": eri_t, "gemm_seconds": gemm_t,
+            "hermite_dmma_tflop": float(stats[-1][608]) / 1e12}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         cpu = cpu_baseline_c1()

@@ -25,7 +25,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
           "-I", str(HERE.parent / "include"), "-I", str(CSRC)]
 SOURCES = ["eri_kernels.cu", "eri_classes_a.cu", "eri_kf_a.cu", "eri_kf_b.cu", "eri_kf_c.cu", "eri_kf_d.cu",
            "grad_kernels.cu", "grad_pot_a.cu", "grad_pot_b.cu", "grad_pot_c.cu",
-           "chol_kernels.cu", "mo_gemm.cu", "gci_api.cu", "host_math.cpp"]
+           "eri_hm_vectors.cu", "eri_hm_0.cu", "eri_hm_1.cu", "eri_hm_2.cu", "eri_hm_3.cu",
+           "eri_hm_4.cu", "eri_hm_5.cu", "eri_hm_6.cu", "chol_kernels.cu", "mo_gemm.cu", "gci_api.cu", "host_math.cpp"]
 # ptxas at -O3 keeps the largest unrolled potential kernels (level sums >= 8)
 # entirely in local memory; -O1 allocates registers for them
 EXTRA = {"grad_pot_b.cu": ["-Xptxas", "-O1"], "grad_pot_c.cu": ["-Xptxas", "-O1"]}

@@ -136,10 +136,16 @@ struct DVec {
 };
 
 // ------------------------------------------------------------------ context
+constexpr int kAuxStreams = 4;
 struct Context {
     bool ready = false;
     int device = 0;
     cudaStream_t stream = nullptr;
+    // streams on which independent class launches of one ERI stage overlap
+    // (forked from and joined back into `stream` by events), created on first use
+    cudaStream_t aux[kAuxStreams] = {};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[kAuxStreams] = {};
     cublasHandle_t blas = nullptr;
     cusolverDnHandle_t solver = nullptr;
     DVec<double> boys;
@@ -399,6 +405,20 @@ struct Handle {
     double eri_stats[kNumPairTypes][kNumPairTypes][kNumStats] = {};
     // scratch reused across ERI launches
     DVec<int> d_bra, d_ket;
+    // Hermite-matrix path: row vectors of every pair that entered a product
+    // stage (offsets by pair id, -1 = not built) and the per-call column data
+    std::vector<int64_t> hm_rowoff_h;
+    DVec<int64_t> hm_rowoff;
+    DVec<double> hm_rowvec;
+    DVec<int> hm_ids;
+    DVec<HmChunk> hm_chunks;
+    DVec<int> hm_colfun, hm_colout, hm_chunkids;
+    DVec<double> hm_colvec;
+    DVec<unsigned long long> hm_counters;
+    double hm_flops = 0.0;
+    // per Hermite-matrix class (L1, L2, column tiles): launches, device seconds
+    // (profiling mode only) and DMMA flops issued
+    double hm_class[kMaxPairL + 1][kMaxPairL + 1][kHmMaxNT][3] = {};                 // DMMA arithmetic issued by the Hermite-matrix kernels (padding included)
 };
 
 // Primitive pairs whose weight |c_a c_b| K_ab (pi/P)^{3/2} (1+|PA|)^la (1+|PB|)^lb is
@@ -506,11 +526,205 @@ static void setup_pairs(Handle& H)
     CU(pair_records_launch(P.d.p, (int)P.n, D.xyz.p, D.poff.p, D.exps.p, D.coefs.p, P.plist.p, P.pp.p, C.stream));
 }
 
+// Hermite-matrix path switch (gci_eri_hm); used for spherical bases in the
+// product and dense modes.
+static std::atomic<int> g_hm_enabled{1};
+// profiling mode (gci_eri_hm(2)): class launches run one after another on the
+// context stream, each bracketed by events, and their times are kept per class
+static std::atomic<int> g_hm_profile{0};
+
+// Row vectors of `ids` (and of every pair built before) in H.hm_rowvec.
+static void hm_ensure_rows(Handle& H, const std::vector<int>& ids)
+{
+    Context& C = ctx();
+    const PairTable& P = H.pt;
+    if ((int64_t)H.hm_rowoff_h.size() != P.n) H.hm_rowoff_h.assign(P.n, -1);
+    bool missing = false;
+    for (int id : ids)
+        if (H.hm_rowoff_h[id] < 0) { missing = true; break; }
+    if (!missing) return;
+    std::vector<char> want(P.n, 0);
+    for (int64_t id = 0; id < P.n; ++id) want[id] = H.hm_rowoff_h[id] >= 0;
+    for (int id : ids) want[id] = 1;
+    std::vector<int> list;
+    std::vector<int64_t> off(P.n, 0);
+    int64_t tot = 0;
+    for (int64_t id = 0; id < P.n; ++id) {
+        if (!want[id]) continue;
+        list.push_back((int)id);
+        off[id] = tot;
+        tot += (int64_t)P.h[id].npp * hm_row_stride(P.h[id].l1 + P.h[id].l2);
+    }
+    H.hm_rowvec.alloc((size_t)std::max<int64_t>(tot, 1));
+    H.hm_rowoff.upload(off, C.stream);
+    H.hm_ids.upload(list, C.stream);
+    CU(hm_rowvec_launch(H.hm_ids.p, (int)list.size(), P.d.p, P.pp.p, H.hm_rowoff.p, H.db.tmat.p, H.db.toff.p,
+                        H.db.nfunc.p, H.hm_rowvec.p, C.stream));
+    for (int64_t id = 0; id < P.n; ++id) H.hm_rowoff_h[id] = want[id] ? off[id] : -1;
+}
+
+// Product / dense stage on the Hermite-matrix kernels.  gb/sb: row pairs
+// grouped by pair type (already on the device in H.d_bra); gk/sk: column
+// pairs grouped by type; `cols` gives the requested columns of each column
+// pair (entries >= 0) and their output column or j index.
+static void run_eri_hm(Handle& H, const std::vector<int>& gb, const std::vector<int64_t>& sb,
+                       const std::vector<int>& gk, const std::vector<int64_t>& sk, int mode, PairMap* rows,
+                       PairMap* cols, double* out, int64_t ldo, int64_t jcount)
+{
+    Context& C = ctx();
+    const PairTable& P = H.pt;
+    hm_ensure_rows(H, gb);
+    // column chunks of at most 8 kHmMaxNT columns, grouped by (column type, tiles)
+    std::vector<HmChunk> chunks;
+    std::vector<int> colfun, colout;
+    std::vector<std::vector<int>> group((size_t)kNumPairTypes * kHmMaxNT);
+    int64_t voff = 0;
+    std::vector<int> fl, ol;
+    for (int tk = 0; tk < kNumPairTypes; ++tk)
+        for (int64_t q = sk[tk]; q < sk[tk + 1]; ++q) {
+            const int id = gk[q];
+            const int nab = P.nab[id];
+            const int* m = cols->map.data() + cols->off[id];
+            fl.clear(); ol.clear();
+            for (int f = 0; f < nab; ++f)
+                if (m[f] >= 0) { fl.push_back(f); ol.push_back(m[f]); }
+            const int n = (int)fl.size();
+            if (n == 0) continue;
+            const int nch = (n + 8 * kHmMaxNT - 1) / (8 * kHmMaxNT);
+            const ShellPairDev& d = P.h[id];
+            const int L = d.l1 + d.l2;
+            for (int c = 0, beg = 0; c < nch; ++c) {
+                const int cnt = n / nch + (c < n % nch ? 1 : 0);
+                HmChunk ch{};
+                ch.pair = id;
+                ch.ncol = cnt;
+                ch.nt = (cnt + 7) / 8;
+                ch.vec_off = voff;
+                ch.col_off = (int64_t)colfun.size();
+                voff += (int64_t)d.npp * hm_col_stride(L, ch.nt);
+                for (int j = beg; j < beg + cnt; ++j) { colfun.push_back(fl[j]); colout.push_back(ol[j]); }
+                beg += cnt;
+                group[(size_t)tk * kHmMaxNT + ch.nt - 1].push_back((int)chunks.size());
+                chunks.push_back(ch);
+            }
+        }
+    if (chunks.empty()) return;
+    std::vector<int> order;
+    std::vector<int64_t> gstart(group.size() + 1, 0);
+    for (size_t g = 0; g < group.size(); ++g) {
+        gstart[g] = (int64_t)order.size();
+        order.insert(order.end(), group[g].begin(), group[g].end());
+    }
+    gstart[group.size()] = (int64_t)order.size();
+    H.hm_chunks.upload(chunks, C.stream);
+    H.hm_colfun.upload(colfun, C.stream);
+    H.hm_colout.upload(colout, C.stream);
+    H.hm_chunkids.upload(order, C.stream);
+    H.hm_colvec.ensure((size_t)std::max<int64_t>(voff, 1));
+    CU(hm_colvec_launch(H.hm_chunks.p, (int)chunks.size(), P.d.p, P.pp.p, H.hm_colfun.p, H.db.tmat.p, H.db.toff.p,
+                        H.db.nfunc.p, H.hm_colvec.p, C.stream));
+    HmArgs a{};
+    a.pairs = P.d.p;
+    a.pp = P.pp.p;
+    a.rowvec = H.hm_rowvec.p;
+    a.rowvec_off = H.hm_rowoff.p;
+    a.chunks = H.hm_chunks.p;
+    a.colvec = H.hm_colvec.p;
+    a.colout = H.hm_colout.p;
+    a.mode = mode;
+    a.out = out;
+    a.ldo = ldo;
+    a.row_off = rows ? rows->doff.p : nullptr;
+    a.row_map = rows ? rows->dmap.p : nullptr;
+    a.sh_nfunc = H.db.nfunc.p;
+    a.sh_loc = H.db.loc.p;
+    a.nao = H.hb.nao;
+    a.jcount = jcount;
+    a.kappa = H.kappa;
+    a.boys = g_ctx.boys.p;
+    // one task counter per launch
+    int64_t nlaunch = 0;
+    for (int tb = 0; tb < kNumPairTypes; ++tb)
+        if (sb[tb + 1] > sb[tb])
+            for (size_t g = 0; g < group.size(); ++g) nlaunch += gstart[g + 1] > gstart[g] ? 1 : 0;
+    if (nlaunch == 0) return;
+    H.hm_counters.ensure((size_t)nlaunch);
+    CU(cudaMemsetAsync(H.hm_counters.p, 0, sizeof(unsigned long long) * nlaunch, C.stream));
+    // the class launches are independent (disjoint outputs): fork them over the auxiliary streams
+    if (!C.ev_fork) {
+        CU(cudaEventCreateWithFlags(&C.ev_fork, cudaEventDisableTiming));
+        for (int q = 0; q < kAuxStreams; ++q) {
+            CU(cudaStreamCreateWithFlags(&C.aux[q], cudaStreamNonBlocking));
+            CU(cudaEventCreateWithFlags(&C.ev_join[q], cudaEventDisableTiming));
+        }
+    }
+    CU(cudaEventRecord(C.ev_fork, C.stream));
+    for (int q = 0; q < kAuxStreams; ++q) CU(cudaStreamWaitEvent(C.aux[q], C.ev_fork, 0));
+    const bool prof = g_hm_profile.load() != 0;
+    std::vector<std::pair<double*, std::pair<cudaEvent_t, cudaEvent_t>>> timed;
+    int64_t li = 0;
+    for (int tb = 0; tb < kNumPairTypes; ++tb) {
+        const int64_t nb = sb[tb + 1] - sb[tb];
+        if (nb == 0) continue;
+        const int L1 = type_lsum(tb);
+        double npb = 0.0, rowt = 0.0;
+        for (int64_t q = sb[tb]; q < sb[tb + 1]; ++q) {
+            const int id = gb[q];
+            npb += P.h[id].npp;
+            rowt += (double)P.h[id].npp * ((P.nab[id] + 7) / 8);
+        }
+        for (int tk = 0; tk < kNumPairTypes; ++tk)
+            for (int nt = 1; nt <= kHmMaxNT; ++nt) {
+                const size_t g = (size_t)tk * kHmMaxNT + nt - 1;
+                const int64_t nc = gstart[g + 1] - gstart[g];
+                if (nc == 0) continue;
+                const int L2 = type_lsum(tk);
+                double npk = 0.0;
+                for (int64_t q = gstart[g]; q < gstart[g + 1]; ++q) npk += P.h[chunks[order[q]].pair].npp;
+                const double fl = 512.0 * nt * (npb * npk * hm_mt(L1) * hm_kt(L2) + rowt * nc * 2.0 * hm_mt(L1));
+                H.hm_flops += fl;
+                double* cs = H.hm_class[L1][L2][nt - 1];
+                cs[0] += 1.0;
+                cs[2] += fl;
+                a.rows = H.d_bra.p + sb[tb];
+                a.nrows = nb;
+                a.chunk_ids = H.hm_chunkids.p + gstart[g];
+                a.nchunks = nc;
+                a.counter = H.hm_counters.p + li;
+                if (prof) {
+                    cudaEvent_t e0, e1;
+                    CU(cudaEventCreate(&e0));
+                    CU(cudaEventCreate(&e1));
+                    CU(cudaEventRecord(e0, C.stream));
+                    CU(hm_launch(L1, L2, nt, a, C.stream));
+                    CU(cudaEventRecord(e1, C.stream));
+                    timed.push_back({cs, {e0, e1}});
+                } else {
+                    CU(hm_launch(L1, L2, nt, a, C.aux[li % kAuxStreams]));
+                }
+                ++li;
+            }
+    }
+    for (int q = 0; q < kAuxStreams; ++q) {
+        CU(cudaEventRecord(C.ev_join[q], C.aux[q]));
+        CU(cudaStreamWaitEvent(C.stream, C.ev_join[q], 0));
+    }
+    for (auto& t : timed) {
+        float ms = 0.f;
+        CU(cudaEventSynchronize(t.second.second));
+        CU(cudaEventElapsedTime(&ms, t.second.first, t.second.second));
+        t.first[1] += ms * 1e-3;
+        cudaEventDestroy(t.second.first);
+        cudaEventDestroy(t.second.second);
+    }
+}
+
 static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<int>& ket, int mode, PairMap* rows,
                     PairMap* cols, double* out, int64_t ldo, int64_t jcount)
 {
     Context& C = ctx();
     const PairTable& P = H.pt;
+    const bool hm = g_hm_enabled.load() && H.hb.spher && mode != kModeDiagonal;
     // class-sorted task lists: pairs grouped by type
     std::vector<int> gb, gk;
     std::vector<int64_t> sb(kNumPairTypes + 1, 0), sk(kNumPairTypes + 1, 0);
@@ -601,9 +815,10 @@ static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<in
             a.nbra = nb;
             a.nket = nk;
             a.swap_bk = tb < tk ? 1 : 0;
-            CU(eri_launch(std::max(tb, tk), std::min(tb, tk), a, C.stream));
+            if (!hm) CU(eri_launch(std::max(tb, tk), std::min(tb, tk), a, C.stream));
         }
     }
+    if (hm) run_eri_hm(H, gb, sb, gk, sk, mode, rows, cols, out, ldo, jcount);
 }
 
 // ------------------------------------------------------------------ step 1
@@ -1634,7 +1849,9 @@ int gci_stats(const gci_handle* h, double* out, int n)
     if (!h || !out) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
     const Handle& H = h->h;
     constexpr int ns = Handle::kNumStats;
-    std::vector<double> v(8 + ns * kNumPairTypes * kNumPairTypes, 0.0);
+    // [8 + ns * 100]: DMMA arithmetic issued by the Hermite-matrix kernels (flops, padding included)
+    std::vector<double> v(8 + ns * kNumPairTypes * kNumPairTypes + 1, 0.0);
+    v[8 + ns * kNumPairTypes * kNumPairTypes] = H.hm_flops;
     for (int i = 0; i < kNumGemm; ++i) v[i] = H.gemm_flops[i];
     for (int tb = 0; tb < kNumPairTypes; ++tb)
         for (int tk = 0; tk < kNumPairTypes; ++tk)
@@ -1752,6 +1969,25 @@ int gci_eri_pairs(const gci_basis* basis, double omega, double* out, int64_t ld)
         CU(cudaMemcpyAsync(out, d.p, sizeof(double) * ld * npq, cudaMemcpyDeviceToHost, C.stream));
         CU(cudaStreamSynchronize(C.stream));
     });
+}
+
+int gci_eri_hm(int enable)
+{
+    const int prev = g_hm_enabled.load() ? (g_hm_profile.load() ? 2 : 1) : 0;
+    if (enable >= 0) {
+        g_hm_enabled.store(enable ? 1 : 0);
+        g_hm_profile.store(enable == 2 ? 1 : 0);
+    }
+    return prev;
+}
+
+int gci_eri_hm_stats(const gci_handle* h, double* out, int n)
+{
+    if (!h || !out) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    const double* v = &h->h.hm_class[0][0][0][0];
+    const int tot = (kMaxPairL + 1) * (kMaxPairL + 1) * kHmMaxNT * 3;
+    for (int i = 0; i < n && i < tot; ++i) out[i] = v[i];
+    return GCI_OK;
 }
 
 int gci_eri_variant(int tb, int tk, int variant)

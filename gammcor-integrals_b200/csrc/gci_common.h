@@ -35,6 +35,13 @@ GCI_HD constexpr int cart_pos(int ly, int lz) { return (ly + lz) * (ly + lz + 1)
 // Shell pair type for l_hi >= l_lo: 0..9 for l <= 3.
 GCI_HD constexpr int pair_type(int lhi, int llo) { return lhi * (lhi + 1) / 2 + llo; }
 constexpr int kNumPairTypes = pair_type(kMaxL, kMaxL) + 1;
+// Hermite level l_hi + l_lo of pair type t.
+GCI_HD constexpr int type_lsum(int t)
+{
+    int hi = 0;
+    while (pair_type(hi + 1, 0) <= t) ++hi;
+    return hi + (t - pair_type(hi, 0));
+}
 
 // Two-centre Hermite coefficients E^{ij}_t of (x-A)^i (x-B)^j exp(-p (x-P)^2),
 // i <= la, j <= lb, t <= i+j, one table per axis: block (i, j) starts at
@@ -133,6 +140,63 @@ struct EriArgs {
     double kappa;
     const double* boys;       // (kBoysMaxM+1) x kBoysNInt x 5
     int* err;                 // device error word
+};
+
+// ------------------------------------------------------------ Hermite-matrix ERI path (eri_hermite.cuh)
+// Largest number of spherical functions of a shell pair of Hermite level L
+// (la + lb = L, la >= lb, la <= kMaxL).
+GCI_HD constexpr int hm_max_nf(int L)
+{
+    int m = 0;
+    for (int la = 0; la <= kMaxL; ++la) {
+        const int lb = L - la;
+        if (lb < 0 || lb > la) continue;
+        const int n = (2 * la + 1) * (2 * lb + 1);
+        if (n > m) m = n;
+    }
+    return m;
+}
+GCI_HD constexpr int hm_mt(int L) { return (herm_n(L) + 7) / 8; }    // 8-row tiles over a Hermite index
+GCI_HD constexpr int hm_kt(int L) { return (herm_n(L) + 3) / 4; }    // 4-wide k-steps over a Hermite index
+GCI_HD constexpr int hm_mto(int L) { return (hm_max_nf(L) + 7) / 8; } // 8-row tiles over the row functions
+// doubles of one row primitive pair's vectors: [MTO][2 MT][32] (A fragments of the row product)
+GCI_HD constexpr int hm_row_stride(int L) { return hm_mto(L) * 2 * hm_mt(L) * 32; }
+// doubles of one column primitive pair's vectors in a chunk of NT column tiles: [KT][NT][32]
+GCI_HD constexpr int hm_col_stride(int L, int nt) { return hm_kt(L) * nt * 32; }
+constexpr int kHmMaxNT = 3;   // column tiles per task (24 columns)
+
+// A group of at most 8 * NT requested columns of one column pair.
+struct HmChunk {
+    int pair;          // pair id (all-pair index)
+    int ncol;          // columns in the chunk
+    int nt;            // column tiles of its vectors (ncol <= 8 nt)
+    int64_t vec_off;   // offset (doubles) of the chunk's vectors in colvec: [k][KT][NT][32]
+    int64_t col_off;   // offset of the chunk's entries in colfun / colout
+};
+
+struct HmArgs {
+    const ShellPairDev* pairs;
+    const double* pp;            // primitive-pair records (P and the product centre at [0..3])
+    const double* rowvec;        // row vectors, per pair: [i][MTO][2 MT][32]
+    const int64_t* rowvec_off;   // per pair id
+    const HmChunk* chunks;
+    const double* colvec;
+    const int* colout;           // per chunk column: output column (product) or j index (dense)
+    const int* rows;             // row pair ids
+    int64_t nrows;
+    const int* chunk_ids;        // chunk indices of this launch
+    int64_t nchunks;
+    int mode;                    // kModeProduct or kModeDense
+    double* out;
+    int64_t ldo;
+    const int64_t* row_off;      // product mode: row map of each row pair (stored-orientation functions)
+    const int* row_map;
+    const int* sh_nfunc;
+    const int* sh_loc;
+    int64_t nao, jcount;
+    double kappa;
+    const double* boys;
+    unsigned long long* counter;   // task counter of the launch, zero at launch
 };
 
 // ------------------------------------------------------------ adjoint (Coulomb gradient) path

@@ -19,6 +19,16 @@ int eri_set_variant(int tb, int tk, int variant);
 cudaError_t pair_records_launch(const ShellPairDev* pairs, int npairs, const double* xyz, const int* poff,
                                 const double* exps, const double* coefs, const int* plist, double* pp,
                                 cudaStream_t st);
+// Hermite-matrix ERI path (eri_hermite.cuh, eri_hm_vectors.cu): row vectors of
+// the listed pairs at offsets off[id], column vectors of the chunks, and the
+// product kernel of row level L1, column level L2 and nt column tiles.
+cudaError_t hm_rowvec_launch(const int* ids, int nids, const ShellPairDev* pairs, const double* pp,
+                             const int64_t* off, const double* tmat, const int* toff, const int* nfunc, double* vec,
+                             cudaStream_t st);
+cudaError_t hm_colvec_launch(const HmChunk* chunks, int nchunks, const ShellPairDev* pairs, const double* pp,
+                             const int* colfun, const double* tmat, const int* toff, const int* nfunc, double* vec,
+                             cudaStream_t st);
+cudaError_t hm_launch(int L1, int L2, int nt, const HmArgs& a, cudaStream_t st);
 cudaError_t boys_eval_launch(int m, int64_t n, const double* x, const double* table, double* out, cudaStream_t st);
 
 cudaError_t launch_segmax(const double* D, const int64_t* loc, const int* dim, int64_t n, double* out, cudaStream_t s);

@@ -183,6 +183,25 @@ int gci_eri_pairs(const gci_basis *basis, double omega, double *out, int64_t ld)
  * process-wide. */
 int gci_eri_variant(int tb, int tk, int variant);
 
+/* Hermite-matrix ERI kernels (default on).  For spherical bases the
+ * product-mode stages (step-1 pivot columns, the pivot block, the
+ * full-dimension stage, gci_eri_pairs) contract each pair's primitive
+ * Hermite coefficients with the normalised solid-harmonic transforms once,
+ * and evaluate every primitive quartet as dense FP64 tensor-core products
+ * (the columns a stage keeps times the Hankel matrix R(h + g)).  The class
+ * kernels above remain for the diagonal stage and Cartesian bases.
+ * enable: 1 on, 0 off, 2 on with per-class timing (the class launches then
+ * run one after another, each timed with CUDA events), < 0 query only;
+ * returns the previous setting.  Process-wide. */
+int gci_eri_hm(int enable);
+
+/* Work of the Hermite-matrix kernels of a decomposition (and its gci_rkab
+ * calls): for every row level L1 (0..6), column level L2 (0..6) and column
+ * tile count (1..3), in that order: launches, device seconds (measured only
+ * with gci_eri_hm(2)) and tensor-core flops issued (padding included);
+ * 7 x 7 x 3 x 3 values. */
+int gci_eri_hm_stats(const gci_handle *h, double *out, int n);
+
 /* Autotuner: times every variant of every class that occurs in `basis` on a
  * product-mode sample of its shell pairs (up to max_pairs bra and max_pairs
  * ket pairs per class) with CUDA events and keeps the fastest.  If
