@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--tune-pairs", type=int, default=40, help="shell pairs per class sampled by the ERI autotuner")
     ap.add_argument("--eri-kernels", default="hermite", choices=["hermite", "class"],
                     help="product stages on the Hermite-matrix tensor-core kernels or the per-class kernels")
+    ap.add_argument("--dump-work", action="store_true",
+                    help="record the job's per-class work counts in oracle/job_work.json (reference-arm input)")
     ap.add_argument("--hm-profile", action="store_true",
                     help="diagnostic: time every Hermite-matrix class launch (serialised) and print the table")
     ap.add_argument("--streams", type=int, default=32, help="c3: workers (CUDA streams) of gci_rkpq_batch")
@@ -148,73 +150,195 @@ def measured_fp64_peak(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_baseline_c1():
-    """The oracle (FP64 C restatement, all host threads) on the full c1 job."""
+WORK_FIXTURE = ROOT / "oracle" / "job_work.json"
+
+
+def job_work(config: str):
+    """Per-class work of the library's job on `config` (gci_stats layout), recorded by
+    ``bench.py --config <cfg> --dump-work`` on a B200 and committed in oracle/job_work.json:
+    the counts the oracle's time is extrapolated over.  None if not recorded."""
+    if not WORK_FIXTURE.exists():
+        return None
+    d = json.loads(WORK_FIXTURE.read_text())
+    w = d.get(config)
+    return None if w is None else np.asarray(w["stats"], dtype=np.float64)
+
+
+def oracle_job_seconds(config: str, work, budget_s: float, rates=None, nthreads: int = 0, seed: int = 0):
+    """Time of the complete `config` job on the oracle (FP64 C restatement of the
+    reference algorithm, scheme 0 = W-matrix + HRR, all host threads), extrapolated
+    from a bounded sample: every ERI class of the job is timed on a seeded sample of
+    its shell quartets from the same molecule, and the job's count of primitive
+    quartets of that class (all of them, as the reference evaluates) is multiplied by
+    the measured seconds per primitive quartet; the GEMM work of the job is timed as
+    numpy DGEMM (OpenBLAS) flops.  `rates` (s per primitive quartet per class, from a
+    previous call) sizes the sample to about `budget_s` seconds.
+    Returns (seconds, rates, sample description)."""
     from gammcor_integrals_b200 import flops, molecules
+    from oracle import oracle as O
+    m = molecules.config(config)
+    ob = O.make_basis(m.atoms, m.shells)
+    O.set_eri_scheme(0)
+    Ls = np.array([sh[1] for sh in m.shells])
+    nprim = np.array([len(sh[2]) for sh in m.shells])
+    byl = {l: np.flatnonzero(Ls == l) for l in range(4)}
+    types = flops.pair_types(3)
+    ntypes, nc = flops.LAYOUTS["lib"]
+    rng = np.random.default_rng(1000 + seed)
+    classes = []
+    for tb in range(ntypes):
+        for tk in range(tb + 1):
+            cnt = work[8 + nc * (tb * ntypes + tk) + 3]
+            if cnt > 0:
+                classes.append((tb, tk, cnt))
+    new_rates, t_eri, n_q = {}, 0.0, 0
+    for tb, tk, cnt in classes:
+        (la, lb), (lc, ld) = types[tb], types[tk]
+        if rates is None:
+            nq = 2
+        else:
+            # this class's share of the budget, in quartets of its mean primitive count
+            share = cnt * rates[(tb, tk)] / sum(c * rates[(b, k)] for b, k, c in classes)
+            mean_pq = np.mean(nprim[byl[la]]) * np.mean(nprim[byl[lb]]) * np.mean(nprim[byl[lc]]) * \
+                np.mean(nprim[byl[ld]])
+            nq = int(np.clip(budget_s * share / (rates[(tb, tk)] * mean_pq), 2, 20000))
+        q = np.stack([rng.choice(byl[la], nq), rng.choice(byl[lb], nq), rng.choice(byl[lc], nq),
+                      rng.choice(byl[ld], nq)], axis=1).astype(np.int32)
+        pq = float(np.sum(np.prod(nprim[q], axis=1)))
+        t0 = time.perf_counter()
+        O.eri_quartets_batch(ob, q, 0.0, nthreads)
+        dt = time.perf_counter() - t0
+        new_rates[(tb, tk)] = dt / pq
+        t_eri += cnt * dt / pq
+        n_q += nq
+    O.set_eri_scheme(1)
+    gemm = float(np.sum(work[:5]))
+    n = 2048
+    a = np.random.default_rng(7).standard_normal((n, n))
+    a @ a
+    t0 = time.perf_counter()
+    a @ a
+    gemm_rate = 2.0 * n ** 3 / (time.perf_counter() - t0)
+    total = t_eri + gemm / gemm_rate
+    desc = (f"{n_q} shell quartets over {len(classes)} ERI classes of the {config} molecule timed on the oracle "
+            f"(W-matrix + HRR route, {os.cpu_count()} threads), extrapolated over the job's primitive-quartet "
+            f"counts per class; GEMM work {gemm / 1e12:.1f} TFLOP at the host DGEMM rate {gemm_rate / 1e9:.0f} GFLOP/s")
+    return total, new_rates, desc
+
+
+def cpu_baseline(config: str, budget_s: float = 20.0):
+    """Reported CPU baseline of our line: the oracle's extrapolated time of the whole
+    job (c1: the full job, measured)."""
+    from gammcor_integrals_b200 import molecules
+    if config == "c1":
+        t, desc = oracle_full_c1()
+    else:
+        work = job_work(config)
+        if work is None:
+            return None
+        _, rates, _ = oracle_job_seconds(config, work, budget_s)
+        t, _, desc = oracle_job_seconds(config, work, budget_s, rates)
+    return {"value": t, "unit": "s", "cores": os.cpu_count(), "kind": "port", "sample": desc}
+
+
+def oracle_full_c1():
+    """The full c1 job on the oracle (decomposition + AO->MO), measured."""
+    from gammcor_integrals_b200 import molecules
     from oracle import oracle as O
     m = molecules.config("c1")
     b = O.make_basis(m.atoms, m.shells)
-    O.stats_reset()
-    t0 = time.perf_counter()
-    ch = O.cholesky(b, m.tau)
     nocc, nvirt, seed = molecules.MO_SPLIT["c1"]
     Cm = molecules.mo_coefficients(b.nao, seed)
+    t0 = time.perf_counter()
+    ch = O.cholesky(b, m.tau)
     O.mo_transf(ch, b, Cm, 0, nocc - 1, Cm, nocc, nocc + nvirt - 1)
     dt = time.perf_counter() - t0
+    nv = ch.nvecs
     O.free(ch)
-    f = flops.job_flops(O.stats(), "oracle")
-    return {"value": f["total"] / dt / 1e9, "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"full c1 job (10 atoms, NAO={b.nao}, {ch.nvecs} vectors, MO 20x60) in {dt:.1f} s "
-                      f"on the oracle (FP64 C restatement of the reference, OpenMP)",
-            "seconds": dt}
+    return dt, (f"full c1 job (NAO={b.nao}, {nv} vectors, MO {nocc}x{nvirt}) on the oracle "
+                f"(FP64 C restatement, OpenMP {os.cpu_count()} threads), measured")
 
 
 def run_reference(args, rank):
-    """--impl reference: the oracle on a bounded sample of the same workload."""
+    """--impl reference: the CPU restatement of the reference algorithm (oracle/) on
+    the same workload as our arm; each step times a bounded sample (c1: the whole
+    job) and reports the job's seconds."""
     if rank != 0:
         return
     import gammcor_pkg
     gammcor_pkg.load()
-    from gammcor_integrals_b200 import flops, molecules
-    from oracle import oracle as O
-    m = molecules.config(args.config)
-    b = O.make_basis(m.atoms, m.shells)
-    sample = "c1 full job" if args.config != "c1" else "c1 full job"
-    # c2 and larger: one step = the full c1 job (the diagonal stage of c2 alone takes > 1 min on 8 cores)
-    mol = molecules.config("c1")
-    ob = O.make_basis(mol.atoms, mol.shells)
-    nocc, nvirt, seed = molecules.MO_SPLIT["c1"]
-    Cm = molecules.mo_coefficients(ob.nao, seed)
+    if args.config in ("c3", "c4"):
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference arm times the Cholesky job configs "
+                                                              f"(c1, c2, c2s, c5); {args.config} has its own bench"}))
+        return
+    work = job_work(args.config) if args.config != "c1" else None
+    if args.config != "c1" and work is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"no recorded work counts for {args.config} "
+                                                              f"in oracle/job_work.json"}))
+        return
+    budget = 5.0
+    rates = None
+    desc = ""
 
     def step():
-        O.stats_reset()
-        t0 = time.perf_counter()
-        ch = O.cholesky(ob, mol.tau)
-        O.mo_transf(ch, ob, Cm, 0, nocc - 1, Cm, nocc, nocc + nvirt - 1)
-        dt = time.perf_counter() - t0
-        O.free(ch)
-        return dt, flops.job_flops(O.stats(), "oracle")["total"]
+        nonlocal rates, desc
+        if args.config == "c1":
+            t, desc = oracle_full_c1()
+            return t
+        t, rates, desc = oracle_job_seconds(args.config, work, budget, rates)
+        return t
 
-    for _ in range(max(0, min(args.warmup, 1))):
+    step() if args.config != "c1" else None   # sizes the per-class samples
+    for _ in range(args.warmup):
         step()
-    tt, ff = 0.0, 0.0
-    for _ in range(args.steps):
-        dt, f = step()
-        tt += dt
-        ff += f
-    v = ff / tt / 1e9
+    vals = [step() for _ in range(args.steps)]
+    v = float(np.mean(vals))
     cores = os.cpu_count()
-    line = {"metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": tt / args.steps * 1e3, "higher_is_better": True,
+    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"{sample} (10 atoms, NAO={ob.nao}), bounded sample of {args.config}",
-                       "tau": mol.tau},
-            "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": cores, "kind": "port",
-                             "sample": f"{sample}: oracle (FP64 C restatement, OpenMP {cores} threads); "
-                                       f"the Fortran reference cannot be compiled here"},
-            "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {"workload": workload_name(args.config), "precision": "fp64"},
+            "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": desc},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "step_values_s": vals}
     print(json.dumps(line), flush=True)
+
+
+def mixed_vs_fp64(L, bstruct, c_dev, nao, a0, a1, b0, b1, buffer_mb, state, torch) -> dict:
+    """Largest difference of the MO Cholesky vectors (and of the MO integrals they
+    reconstruct, sampled) between the split-precision and the FP64 path of one job."""
+    import ctypes as C
+    from gammcor_integrals_b200 import _capi
+    from gammcor_integrals_b200 import cholesky_gammcor as cg
+    out = {}
+    h = C.c_void_p()
+    _capi.check(L.gci_rkpq(C.byref(bstruct), cg.CHOL_ACCURACY_TIGHT, 0.0, 0, C.byref(h)))
+    nv = C.c_int64()
+    _capi.check(L.gci_query(h, C.byref(nv), None, None, None, None, None))
+    res = {}
+    for name, prec in (("fp64", _capi.GCI_PREC_FP64), ("mixed", _capi.GCI_PREC_MIXED)):
+        r = torch.empty(nv.value * (a1 - a0 + 1) * (b1 - b0 + 1), dtype=torch.float64, device="cuda")
+        _capi.check(L.gci_rkab_device(h, C.c_void_p(c_dev.data_ptr()), nao, a0, a1, C.c_void_p(c_dev.data_ptr()),
+                                      nao, b0, b1, buffer_mb, prec, C.c_void_p(r.data_ptr())))
+        res[name] = r.view(-1, nv.value)   # (NA*NB, NVecs): column k of vector k
+    L.gci_free(h)
+    d = (res["mixed"] - res["fp64"]).abs().max().item()
+    g = torch.Generator(device="cpu").manual_seed(5)
+    idx = torch.randint(0, res["fp64"].shape[0], (512,), generator=g).cuda()
+    A, B = res["fp64"][idx], res["mixed"][idx]
+    mo = (A @ A.T - B @ B.T).abs().max().item()
+    out["rkab_mixed_vs_fp64"] = d
+    out["mo_integrals_mixed_vs_fp64_sampled"] = mo
+    return out
+
+
+def workload_name(config: str) -> str:
+    from gammcor_integrals_b200 import molecules
+    m = molecules.config(config)
+    nocc, nvirt, _ = molecules.MO_SPLIT.get(config, (20, 60, 101))
+    return (f"{config}: {len(m.atoms)} atoms, NAO={m.nao}, tau={m.tau}, two-step Cholesky of (pq|rs) + "
+            f"AO->MO {nocc}x{nvirt}")
 
 
 def run_grad(args, rank, world, local):
@@ -452,6 +576,8 @@ def main():
     def job():
         h = C.c_void_p()
         flags = _capi.GCI_FLAG_PIVOT_DECODE_STORAGE if args.decode_storage else 0
+        if args.precision == "mixed":
+            flags |= _capi.GCI_FLAG_MIXED_STEP1
         _capi.check(L.gci_rkpq(C.byref(bstruct), cg.CHOL_ACCURACY_TIGHT, 0.0, flags, C.byref(h)))
         nv = C.c_int64()
         _capi.check(L.gci_query(h, C.byref(nv), None, None, None, None, None))
@@ -481,7 +607,7 @@ def main():
     t_dev = 0.0
     with ClockSampler(local) as clk:
         barrier()
-        stats, times = [], []
+        stats, times, step_s = [], [], []
         for _ in range(args.steps):
             with torch.cuda.stream(lib_stream):
                 flush.fill_(1.0)
@@ -491,6 +617,7 @@ def main():
             ev1.record(lib_stream)
             ev1.synchronize()
             t_dev += ev0.elapsed_time(ev1) * 1e-3
+            step_s.append(ev0.elapsed_time(ev1) * 1e-3)
             stats.append(st)
             times.append(tm)
         barrier()
@@ -507,9 +634,21 @@ def main():
         for t, a, b, c, n, f in rows:
             print(f"#  L1={a} L2={b} NT={c}  launches {int(n):5d}  {t:8.3f} s  {100 * t / max(tot, 1e-30):5.1f}%  "
                   f"{f / 1e12:8.2f} TF  {f / max(t, 1e-30) / 1e12:6.2f} TF/s", file=sys.stderr)
+    if args.dump_work and rank == 0:
+        d = json.loads(WORK_FIXTURE.read_text()) if WORK_FIXTURE.exists() else {}
+        d[args.config] = {"how": f"python bench.py --config {args.config} --dump-work on one B200 "
+                                 f"(gci_stats of one job: GEMM flops and per-class ERI counters)",
+                          "nvecs": int(state["nvecs"]), "stats": [float(x) for x in stats[-1]]}
+        WORK_FIXTURE.write_text(json.dumps(d, indent=1) + "\n")
     fl = flops.job_flops(stats[-1], "lib")
     flops_step = fl["total"]
-    value = aggregate_rate(flops_step, args.steps, world, t_max) / 1e9
+    sec = t_max / args.steps
+    # accuracy of this job's results: the FP64 path is checked against the oracle by the
+    # parity tests (tests/test_gpu_parity.py); a split-precision run is compared here
+    # with the FP64 path on the same molecule
+    err = {"fp64_path": "parity with the FP64 oracle: tests/test_gpu_parity.py"}
+    if args.precision != "fp64":
+        err.update(mixed_vs_fp64(L, bstruct, c_dev, nao, a0, a1, b0, b1, args.buffer_mb, state, torch))
 
     # ---- end to end through the public host API (pinned host buffers)
     e2e = None
@@ -522,7 +661,7 @@ def main():
         e0.record(lib_stream)
         for _ in range(args.e2e_steps):
             res = cg.chol_gammcor_Rkpq(tb, cg.CHOL_ACCURACY_TIGHT, materialize=False,
-                                       decode_storage=args.decode_storage)
+                                       decode_storage=args.decode_storage, mixed_step1=args.precision == "mixed")
             _capi.check(L.gci_rkab(res.handle.ptr, _capi.ptr(pin_c.numpy()), nao, a0, a1, _capi.ptr(pin_c.numpy()),
                                    nao, b0, b1, args.buffer_mb, prec, _capi.ptr(pin_out.numpy())))
             checksum = float(pin_out[:16].sum())
@@ -532,9 +671,8 @@ def main():
         te = max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, "cuda")
         h2d = int(Cm.nbytes) + int(tb.CntrCoeffs.nbytes + tb.Exponents.nbytes + tb.AtomCoords.nbytes)
         d2h = nv * NA * NB * 8
-        e2e = {"value": aggregate_rate(flops_step, args.e2e_steps, world, te) / 1e9, "unit": "GFLOP/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "seconds_per_step": te / args.e2e_steps,
-               "checksum": checksum}
+        e2e = {"value": te / args.e2e_steps, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "gflops": aggregate_rate(flops_step, args.e2e_steps, world, te) / 1e9, "checksum": checksum}
 
     if rank != 0:
         if world > 1:
@@ -546,35 +684,38 @@ def main():
     eri_t = tm[0] + tm[1] + tm[5] + tm[7]
     gemm_t = tm[2] + tm[8] + tm[9]
     peak64 = measured_fp64_peak(torch)
-    variants = {(tb_, tk_): L.gci_eri_variant(tb_, tk_, -1) for tb_ in range(10) for tk_ in range(tb_ + 1)}
-    kflops = flops.kernel_flops(stats[-1], variants)
-    eri_rate = kflops / eri_t / 1e12 if eri_t > 0 else 0.0
-    roof = {"bound": "fp64", "kernel": "k_eri_kf / k_eri_class (all ERI stages, per-class variant)",
-            "achieved": eri_rate, "peak": peak64,
-            "unit": "TFLOP/s", "frac": eri_rate / peak64 if peak64 else None, "traffic": None,
+    eri_alg = flops.eri_flops(stats[-1], "lib", unscreened=False)
+    hm_issued = float(stats[-1][608])
+    roof = {"bound": "fp64", "kernel": "k_eri_hm (Hermite-matrix ERI kernels, FP64 tensor cores) + the diagonal "
+                                       "stage's class kernels: all ERI stages",
+            "achieved": eri_alg / eri_t / 1e12 if eri_t > 0 else 0.0, "peak": peak64, "unit": "TFLOP/s",
+            "frac": (eri_alg / eri_t / 1e12) / peak64 if (peak64 and eri_t > 0) else None, "traffic": None,
+            "achieved_definition": "reference-algorithm ERI flops of the evaluated primitive quartets (flops.py "
+                                   "class_flops) / device seconds of the ERI stages",
             "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64; MEASURED_PEAKS.json has no FP64 figure)",
-            "eri_seconds": eri_t, "gemm_seconds": gemm_t,
-            "hermite_dmma_tflop": float(stats[-1][608]) / 1e12}
+            "issued_tflops_per_s": hm_issued / eri_t / 1e12 if eri_t > 0 else 0.0,
+            "issued_definition": "tensor-core flops the Hermite-matrix kernels issued (padding included)",
+            "eri_seconds": eri_t, "gemm_seconds": gemm_t}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        cpu = cpu_baseline_c1()
-    line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+        cpu = cpu_baseline(args.config)
+    line = {"metric": METRIC, "value": sec, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.config}: {len(mol.atoms)} atoms, NAO={nao}, tau={mol.tau}, "
-                                   f"Cholesky + AO->MO {NA}x{NB}",
-                       "precision": args.precision, "nvecs": state["nvecs"], "parallelism": f"replicas x{world}",
-                       "l2": "flushed before every timed step (512 MB write outside the timed events)",
-                       "eri_autotune": {"seconds": round(t_tune, 2),
-                                        "classes_per_variant": {"team": kf_classes[0], "ket_first_32": kf_classes[1],
-                                                                "ket_first_64": kf_classes[2], "ket_first_128": kf_classes[3]}}},
-            "wall_s_per_step": t_max / args.steps, "gflop_per_step": flops_step / 1e9,
-            "gflop_executed_per_step": fl["executed"] / 1e9,
-            "value_definition": "reference-algorithm work (GEMM formulas + W-matrix ERI arithmetic over every "
-                                "primitive quartet, flops.py) per second of device time",
+            "config": {"workload": workload_name(args.config), "precision": args.precision,
+                       "nvecs": state["nvecs"], "parallelism": f"replicas x{world}",
+                       "l2": "flushed before every timed step (512 MB write outside the timed events)"},
+            "value_definition": "device seconds of one complete job (decomposition + AO->MO) on each GPU, "
+                                "CUDA events on the library stream, max over ranks",
+            "gflops": aggregate_rate(flops_step, args.steps, world, t_max) / 1e9,
+            "gflops_definition": "reference-algorithm work of the job (GEMM formulas + W-matrix ERI arithmetic "
+                                 "over every primitive quartet, flops.py) per second, all ranks",
+            "gflop_per_step": flops_step / 1e9, "gflop_executed_per_step": fl["executed"] / 1e9,
             "eri_per_s": fl["integrals"] * args.steps * world / t_max, "phases_s": phases,
+            "step_seconds": [round(x, 3) for x in step_s],
             "gpu_launches": int(n1.value - n0.value), "roofline": roof, "e2e": e2e,
             "clocks": clk.summary(), "cpu_baseline": cpu}
+    line["max_abs_err"] = err
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

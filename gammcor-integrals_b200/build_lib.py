@@ -1,7 +1,8 @@
 """Build libgci.so (CUDA sm_100a kernels + C ABI) in-tree with nvcc.
 
-Run as a script or call ``build()``; objects go to ``_lib/obj`` and the
-library to ``_lib/libgci.so`` next to this file.  Recompiles only sources
+Run as a script or call ``build()``; objects go to ``_lib/obj``, the shared
+library to ``_lib/libgci.so`` and the same objects as a static archive to
+``_lib/libgci.a`` next to this file.  Recompiles only sources
 newer than their object.
 """
 from __future__ import annotations
@@ -17,6 +18,7 @@ CSRC = HERE / "csrc"
 OUT = HERE / "_lib"
 OBJ = OUT / "obj"
 LIB = OUT / "libgci.so"
+ARCHIVE = OUT / "libgci.a"
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 
@@ -26,7 +28,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
 SOURCES = ["eri_kernels.cu", "eri_classes_a.cu", "eri_kf_a.cu", "eri_kf_b.cu", "eri_kf_c.cu", "eri_kf_d.cu",
            "grad_kernels.cu", "grad_pot_a.cu", "grad_pot_b.cu", "grad_pot_c.cu",
            "eri_hm_vectors.cu", "eri_hm_0.cu", "eri_hm_1.cu", "eri_hm_2.cu", "eri_hm_3.cu",
-           "eri_hm_4.cu", "eri_hm_5.cu", "eri_hm_6.cu", "chol_kernels.cu", "mo_gemm.cu", "gci_api.cu", "host_math.cpp"]
+           "eri_hm_4.cu", "eri_hm_5.cu", "eri_hm_6.cu", "chol_kernels.cu", "ozaki_gemm.cu", "gci_api.cu", "host_math.cpp"]
 # ptxas at -O3 keeps the largest unrolled potential kernels (level sums >= 8)
 # entirely in local memory; -O1 allocates registers for them
 EXTRA = {"grad_pot_b.cu": ["-Xptxas", "-O1"], "grad_pot_c.cu": ["-Xptxas", "-O1"]}
@@ -89,6 +91,15 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if todo or not ARCHIVE.exists():
+        # the same objects as a static archive, for a Fortran build that links the
+        # library into its own cholesky.a-based executable (the caller adds
+        # -lcudart -lcublas -lcusolver -lstdc++)
+        if ARCHIVE.exists():
+            ARCHIVE.unlink()
+        r = subprocess.run(["ar", "rcs", str(ARCHIVE), *map(str, objs)], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"ar failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

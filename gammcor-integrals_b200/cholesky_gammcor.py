@@ -87,12 +87,15 @@ def accuracy_tau(Accuracy: int) -> float:
 
 
 def chol_gammcor_Rkpq(AOBasis: TAOBasis, Accuracy: int, Omega: float | None = None, *, materialize: bool = True,
-                      copy_to_host: bool = True, decode_storage: bool = False) -> TCholeskyVecsOTF:
-    """Cholesky vectors in the AO basis computed on the fly (Cholesky_Gammcor.f90:335-377)."""
+                      copy_to_host: bool = True, decode_storage: bool = False,
+                      mixed_step1: bool = False) -> TCholeskyVecsOTF:
+    """Cholesky vectors in the AO basis computed on the fly (Cholesky_Gammcor.f90:335-377).
+    mixed_step1: M - L L^T of the pivot search as a split-precision int8 tensor-core GEMM."""
     L = _capi.lib()
     b = AOBasis.c_struct()
     flags = (_capi.GCI_FLAG_MATERIALIZE_RKPQ if materialize else 0) | \
-            (_capi.GCI_FLAG_PIVOT_DECODE_STORAGE if decode_storage else 0)
+            (_capi.GCI_FLAG_PIVOT_DECODE_STORAGE if decode_storage else 0) | \
+            (_capi.GCI_FLAG_MIXED_STEP1 if mixed_step1 else 0)
     h = C.c_void_p()
     _capi.check(L.gci_rkpq(C.byref(b), int(Accuracy), float(Omega) if Omega else 0.0, flags, C.byref(h)))
     return _vecs_from_handle(_Handle(h), materialize and copy_to_host)

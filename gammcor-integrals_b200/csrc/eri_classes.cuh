@@ -20,12 +20,9 @@ static void launch_class(const EriArgs& args, cudaStream_t st)
     using G = EriTeam<LA, LB, LC, LD>;
     const size_t smem = G::smem_bytes();
     auto kern = k_eri_class<LA, LB, LC, LD>;
-    // once per kernel, thread-safe (function-local static initialisation)
-    static const bool attr_set = [&] {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        return true;
-    }();
-    (void)attr_set;
+    // the attribute belongs to the current device: set it on every launch, so that
+    // launches on any device the library is called on see it
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int64_t ntasks = (args.mode == kModeDiagonal) ? args.nbra : args.nbra * args.nket;
     if (ntasks <= 0) return;
     int64_t blocks = (ntasks + G::NT - 1) / G::NT;
@@ -47,12 +44,9 @@ static void launch_kf(const EriArgs& args, cudaStream_t st)
     using K = KfShape<LA, LB, LC, LD, TWQ>;
     const size_t smem = K::smem_bytes();
     auto kern = k_eri_kf<LA, LB, LC, LD, TWQ>;
-    // once per kernel, thread-safe (function-local static initialisation)
-    static const bool attr_set = [&] {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        return true;
-    }();
-    (void)attr_set;
+    // the attribute belongs to the current device: set it on every launch, so that
+    // launches on any device the library is called on see it
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int64_t ntasks = (args.mode == kModeDiagonal) ? args.nbra : args.nbra * args.nket;
     if (ntasks <= 0) return;
     int64_t blocks = (ntasks + K::TEAMS - 1) / K::TEAMS;

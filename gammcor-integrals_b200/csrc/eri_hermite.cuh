@@ -29,6 +29,7 @@
 #pragma once
 #include "gci_common.h"
 #include "boys.cuh"
+#include <type_traits>
 
 namespace gci {
 
@@ -46,12 +47,29 @@ struct HmShape {
     // eight warps share the block's tables; (f,f|f,f) with three column tiles
     // fills 226 KB of shared memory
     static constexpr int WARPS = 8, TPB = 32 * WARPS;
+    // independent accumulator sets over alternating k-steps, so that at least
+    // ~12 tensor-core products are in flight per warp when the tile count is small
+    static constexpr int ACC0 = (12 + MT * NT - 1) / (MT * NT);
+    static constexpr int ACC = ACC0 > 4 ? 4 : ACC0;
+    // blocks per SM the launch bounds ask for: two when the accumulators are few
+    static constexpr int MINB = ACC * MT * NT * 2 <= 24 ? 2 : 1;
+    // the next k-step's Hankel fragments are loaded one step ahead (registers: 2 MT)
+    static constexpr bool APF = MT <= 7;
     static constexpr size_t smem_bytes()
     {
         return sizeof(double) * ((size_t)WARPS * WS + HT) + sizeof(int) * (size_t)HT +
                sizeof(short) * (size_t)MT * KT * 32;
     }
 };
+
+template <int I, int N, class Fn>
+__device__ __forceinline__ void hm_static_for(Fn&& fn)
+{
+    if constexpr (I < N) {
+        fn(std::integral_constant<int, I>{});
+        hm_static_for<I + 1, N>(fn);
+    }
+}
 
 // D = A B + D for one 8x8x4 tile: lane l holds A[l/4][l%4], B[l%4][l/4] and
 // D[l/4][2(l%4) + {0,1}].
@@ -88,11 +106,11 @@ __device__ __forceinline__ void hm_level(int j, const double* __restrict__ fk, c
 }
 
 template <int L1, int L2, int NT>
-__global__ void __launch_bounds__(HmShape<L1, L2, NT>::TPB, 1)
+__global__ void __launch_bounds__(HmShape<L1, L2, NT>::TPB, HmShape<L1, L2, NT>::MINB)
 k_eri_hm(const HmArgs a)
 {
     using S = HmShape<L1, L2, NT>;
-    constexpr int LT = S::LT, HT = S::HT, MT = S::MT, KT = S::KT, MTO = S::MTO;
+    constexpr int LT = S::LT, HT = S::HT, MT = S::MT, KT = S::KT, MTO = S::MTO, ACC = S::ACC;
     extern __shared__ double smem[];
     double* tab_coef = smem + (size_t)S::WARPS * S::WS;
     int* tab_rec = reinterpret_cast<int*>(tab_coef + HT);
@@ -154,11 +172,13 @@ k_eri_hm(const HmArgs a)
         for (int i = 0; i < nb; ++i) {
             const double* __restrict__ Bp = rrec + (size_t)i * rsr;
             const double P = __ldg(Bp + 0), px = __ldg(Bp + 1), py = __ldg(Bp + 2), pz = __ldg(Bp + 3);
-            double X[MT][NT][2];
+            double X[ACC][MT][NT][2];
 #pragma unroll
-            for (int m = 0; m < MT; ++m)
+            for (int u = 0; u < ACC; ++u)
 #pragma unroll
-                for (int n = 0; n < NT; ++n) X[m][n][0] = X[m][n][1] = 0.0;
+                for (int m = 0; m < MT; ++m)
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) X[u][m][n][0] = X[u][m][n][1] = 0.0;
 
             for (int k0 = 0; k0 < nk; k0 += S::KB) {
                 const int kn = (nk - k0) < S::KB ? (nk - k0) : S::KB;
@@ -207,29 +227,54 @@ k_eri_hm(const HmArgs a)
                     double bn[NT];
 #pragma unroll
                     for (int n = 0; n < NT; ++n) bn[n] = __ldg(cv + n * 32);
+                    double an[S::APF ? MT : 1];
+                    if constexpr (S::APF) {
+#pragma unroll
+                        for (int m = 0; m < MT; ++m) an[m] = C[tab_gidx[m * KT * 32 + lane]];
+                    }
                     int q = 0;
 #pragma unroll 1
-                    for (int ks = 0; ks < KT; ++ks) {
-                        double b[NT];
+                    for (int ks0 = 0; ks0 < KT; ks0 += ACC) {
+                        hm_static_for<0, ACC>([&](auto U) {
+                            constexpr int u = decltype(U)::value;
+                            const int ks = ks0 + u;
+                            if (ks < KT) {
+                                double b[NT];
 #pragma unroll
-                        for (int n = 0; n < NT; ++n) b[n] = bn[n];
-                        if (ks + 1 < KT) {
+                                for (int n = 0; n < NT; ++n) b[n] = bn[n];
+                                if (ks + 1 < KT) {
 #pragma unroll
-                            for (int n = 0; n < NT; ++n) bn[n] = __ldg(cv + ((ks + 1) * NT + n) * 32);
-                        }
-                        const short* gi = tab_gidx + ks * 32 + lane;
+                                    for (int n = 0; n < NT; ++n) bn[n] = __ldg(cv + ((ks + 1) * NT + n) * 32);
+                                }
+                                const short* gi = tab_gidx + ks * 32 + lane;
+                                if constexpr (S::APF) {
+                                    double av[MT];
 #pragma unroll
-                        for (int m = 0; m < MT; ++m) {
-                            const double av = C[gi[m * KT * 32]];
+                                    for (int m = 0; m < MT; ++m) av[m] = an[m];
+                                    if (ks + 1 < KT) {
 #pragma unroll
-                            for (int n = 0; n < NT; ++n) dmma884(X[m][n], av, b[n]);
-                        }
-                        const int qe = more ? ((ks + 1) * LT) / KT : 0;
-                        for (; q < qe; ++q) {
-                            hm_level<LT>(LT - 1 - q, fkn, src, dst, tab_rec, tab_coef, lane);
-                            __syncwarp();
-                            double* tmp = src; src = dst; dst = tmp;
-                        }
+                                        for (int m = 0; m < MT; ++m) an[m] = C[gi[m * KT * 32 + 32]];
+                                    }
+#pragma unroll
+                                    for (int m = 0; m < MT; ++m)
+#pragma unroll
+                                        for (int n = 0; n < NT; ++n) dmma884(X[u][m][n], av[m], b[n]);
+                                } else {
+#pragma unroll
+                                    for (int m = 0; m < MT; ++m) {
+                                        const double av = C[gi[m * KT * 32]];
+#pragma unroll
+                                        for (int n = 0; n < NT; ++n) dmma884(X[u][m][n], av, b[n]);
+                                    }
+                                }
+                                const int qe = more ? ((ks + 1) * LT) / KT : 0;
+                                for (; q < qe; ++q) {
+                                    hm_level<LT>(LT - 1 - q, fkn, src, dst, tab_rec, tab_coef, lane);
+                                    __syncwarp();
+                                    double* tmp = src; src = dst; dst = tmp;
+                                }
+                            }
+                        });
                     }
                     // the next quartet's R^{(0)} is in src; the free buffers rotate
                     double* tmp = C; C = src; src = tmp;
@@ -238,30 +283,42 @@ k_eri_hm(const HmArgs a)
             }
             // O(r, J) += Er_i(r, h) X(h, J); the B fragment of k-step ks (h = 4 ks + l%4,
             // J = 8 n + l/4) is held by lane 16 (ks%2) + 4 (l%4) + l/8 of X[ks/2][n]
+            if constexpr (ACC > 1) {
+#pragma unroll
+                for (int u = 1; u < ACC; ++u)
+#pragma unroll
+                    for (int m = 0; m < MT; ++m)
+#pragma unroll
+                        for (int n = 0; n < NT; ++n) { X[0][m][n][0] += X[u][m][n][0]; X[0][m][n][1] += X[u][m][n][1]; }
+            }
             const double* __restrict__ rv = rowv + (size_t)i * S::RSTR + lane;
             const int src0 = ((lane & 3) << 2) + (lane >> 3);
             const bool odd = (lane >> 2) & 1;
-            // one 8-row tile of O at a time, accumulated into the warp's block in shared memory
+            // one 8-row tile of O at a time (even and odd k-steps in separate
+            // accumulators), added into the warp's block in shared memory
 #pragma unroll 1
             for (int m = 0; m < MTO; ++m) {
                 if (8 * m >= nR) break;
-                double acc[NT][2];
+                double acc[2][NT][2];
 #pragma unroll
-                for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = 0.0;
+                for (int n = 0; n < NT; ++n) acc[0][n][0] = acc[0][n][1] = acc[1][n][0] = acc[1][n][1] = 0.0;
 #pragma unroll
                 for (int ks = 0; ks < 2 * MT; ++ks) {
                     const double av = __ldg(rv + (m * 2 * MT + ks) * 32);
                     const int srcl = src0 + ((ks & 1) << 4);
 #pragma unroll
                     for (int n = 0; n < NT; ++n) {
-                        const double v0 = __shfl_sync(0xffffffffu, X[ks >> 1][n][0], srcl);
-                        const double v1 = __shfl_sync(0xffffffffu, X[ks >> 1][n][1], srcl);
-                        dmma884(acc[n], av, odd ? v1 : v0);
+                        const double v0 = __shfl_sync(0xffffffffu, X[0][ks >> 1][n][0], srcl);
+                        const double v1 = __shfl_sync(0xffffffffu, X[0][ks >> 1][n][1], srcl);
+                        dmma884(acc[ks & 1][n], av, odd ? v1 : v0);
                     }
                 }
                 double* o = Os + (m * NT) * 64 + 2 * lane;
 #pragma unroll
-                for (int n = 0; n < NT; ++n) { o[n * 64] += acc[n][0]; o[n * 64 + 1] += acc[n][1]; }
+                for (int n = 0; n < NT; ++n) {
+                    o[n * 64] += acc[0][n][0] + acc[1][n][0];
+                    o[n * 64 + 1] += acc[0][n][1] + acc[1][n][1];
+                }
             }
         }
 

@@ -2,6 +2,8 @@
 // kernels, the primitive-pair record kernel and the Boys self-test kernel.
 #include "eri_classes.cuh"
 #include "gci_runtime.h"
+#include <atomic>
+#include <mutex>
 
 namespace gci {
 
@@ -103,7 +105,9 @@ __global__ void k_boys_eval(int m, int64_t n, const double* __restrict__ x, cons
 
 static LaunchFn g_launch[kNumPairTypes][kNumPairTypes];                   // team kernels (bra types up to (d,d))
 static LaunchFn g_launch_kf[kNumKfWidths][kNumPairTypes][kNumPairTypes];  // ket-first kernels where built
-static int g_variant[kNumPairTypes][kNumPairTypes];   // 0 team, 1 + w ket-first of width kf_width(w)
+// 0 team, 1 + w ket-first of width kf_width(w); read by launches and written by the
+// tuner or gci_eri_variant from any thread
+static std::atomic<int> g_variant[kNumPairTypes][kNumPairTypes];
 
 static LaunchFn variant_fn(int tb, int tk, int v)
 {
@@ -112,10 +116,8 @@ static LaunchFn variant_fn(int tb, int tk, int v)
     return nullptr;
 }
 
-cudaError_t eri_module_init()
+static void eri_register()
 {
-    static bool done = false;
-    if (done) return cudaSuccess;
     register_eri_classes_a(g_launch);
     register_eri_kf_a(g_launch_kf);
     register_eri_kf_b(g_launch_kf);
@@ -128,7 +130,12 @@ cudaError_t eri_module_init()
             for (int v = kNumKfWidths; v >= 1; --v)
                 if (variant_fn(tb, tk, v)) g_variant[tb][tk] = v;
         }
-    done = true;
+}
+
+cudaError_t eri_module_init()
+{
+    static std::once_flag once;
+    std::call_once(once, eri_register);
     return cudaSuccess;
 }
 

@@ -4,12 +4,11 @@
 // Control flow follows the reference driver (TwoStepCholesky*.f90,
 // Cholesky_Gammcor.f90); the integral, pivot-search and contraction work
 // runs on the device (eri_kernels.cu, chol_kernels.cu, cuBLAS DGEMM for the
-// FP64 contractions, mo_gemm.cu for the split-precision tensor-core GEMMs).
+// FP64 contractions, ozaki_gemm.cu for the split-precision int8 tensor-core GEMMs).
 #include "../../include/gci.h"
 #include "gci_common.h"
 #include "gci_runtime.h"
 #include "host_math.h"
-#include "mo_gemm.h"
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 #include <algorithm>
@@ -138,7 +137,7 @@ struct DVec {
 // ------------------------------------------------------------------ context
 constexpr int kAuxStreams = 4;
 struct Context {
-    bool ready = false;
+    std::atomic<bool> ready{false};
     int device = 0;
     cudaStream_t stream = nullptr;
     // streams on which independent class launches of one ERI stage overlap
@@ -175,6 +174,10 @@ static Context& ctx()
         t_stream = t_cur->stream;
         return *t_cur;
     }
+    // the process-wide context is created once; concurrent first calls wait here
+    static std::mutex init_mutex;
+    std::unique_lock<std::mutex> init_lock(init_mutex, std::defer_lock);
+    if (!g_ctx.ready) init_lock.lock();
     if (!g_ctx.ready) {
         int ndev = 0;
         cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -840,6 +843,49 @@ static void gemm_nt(cublasHandle_t h, int64_t m, int64_t n, int64_t k, double al
     CB(cublasDgemm_64(h, CUBLAS_OP_N, CUBLAS_OP_T, m, n, k, &alpha, A, lda, B, ldb, &beta, Cm, ldc));
 }
 
+// Split-precision form of C = alpha A B^T + beta C on the int8 tensor cores
+// (ozaki_gemm.cu).  A(i, l) = A[i * ars + l * als], B(j, l) = B[j * brs + l * bls],
+// C column-major.  Rows of A are taken in chunks whose slice tiles fit a ~4 GB
+// workspace, and K in chunks the int32 accumulators hold exactly.
+static void gemm_nt_split(int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t ars, int64_t als,
+                          const double* B, int64_t brs, int64_t bls, double beta, double* Cm, int64_t ldc)
+{
+    if (m == 0 || n == 0) return;
+    Context& C = ctx();
+    if (k == 0) {
+        if (beta == 1.0) return;
+        fail(GCI_ERR_ARG, "split-precision GEMM with k = 0 and beta != 1");
+    }
+    const int64_t kmax = ozaki_max_k();
+    const int64_t kc = std::min<int64_t>(k, kmax);
+    const int64_t per_row = (int64_t)ozaki_workspace_bytes(128, 0, kc) / 128 + 1;
+    int64_t rows = std::max<int64_t>(128, ((int64_t)4 << 30) / per_row / 128 * 128);
+    rows = std::min<int64_t>(rows, (int64_t)65535 * 128);
+    DVec<unsigned char> work;
+    work.alloc(ozaki_workspace_bytes(std::min(rows, m), n, kc));
+    for (int64_t k0 = 0; k0 < k; k0 += kc) {
+        const int64_t kk = std::min(kc, k - k0);
+        const double b = k0 == 0 ? beta : 1.0;
+        for (int64_t r0 = 0; r0 < m; r0 += rows) {
+            const int64_t mm = std::min(rows, m - r0);
+            CU(ozaki_dgemm_nt(mm, n, kk, alpha, A + r0 * ars + k0 * als, ars, als, B + k0 * bls, brs, bls, b,
+                              Cm + r0, ldc, work.p, C.err.p, C.stream));
+        }
+    }
+}
+
+// Error word of the context (set by bounded waits in the kernels that expire).
+static void check_device_error(Context& C, const char* what)
+{
+    int e = 0;
+    CU(cudaMemcpyAsync(&e, C.err.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
+    CU(cudaStreamSynchronize(C.stream));
+    if (e != 0) {
+        CU(cudaMemsetAsync(C.err.p, 0, sizeof(int), C.stream));
+        fail(GCI_ERR_CUDA, std::string(what) + ": a bounded device wait expired");
+    }
+}
+
 static void step1(Handle& H)
 {
     Context& C = ctx();
@@ -1109,7 +1155,10 @@ static void step1(Handle& H)
             if (nchol > 0) {
                 dLB.ensure((size_t)nbatch * nchol);
                 CU(launch_gather_rows(Lst.p, ncand, dbrow.p, nbatch, nchol, dLB.p, nbatch, s));
-                gemm_nt(C.blas, ncand, nbatch, nchol, -1.0, Lst.p, ncand, dLB.p, nbatch, 1.0, dM.p, ncand);
+                if (H.flags & GCI_FLAG_MIXED_STEP1)
+                    gemm_nt_split(ncand, nbatch, nchol, -1.0, Lst.p, 1, ncand, dLB.p, 1, nbatch, 1.0, dM.p, ncand);
+                else
+                    gemm_nt(C.blas, ncand, nbatch, nchol, -1.0, Lst.p, ncand, dLB.p, nbatch, 1.0, dM.p, ncand);
                 H.gemm_flops[kGemmSubtractR] += 2.0 * ncand * nbatch * nchol;
             }
             T.stop();
@@ -1177,6 +1226,7 @@ static void step1(Handle& H)
         if (dmax <= H.tau) { converged = true; go = false; }
         if (nchol == maxnchol || nbatch == 0) go = false;
     }
+    if (H.flags & GCI_FLAG_MIXED_STEP1) check_device_error(C, "split-precision M - L L^T");
     H.nvecs = nchol;
     H.nmacro = nmacro;
     H.converged = converged ? 1 : 0;
@@ -1345,8 +1395,10 @@ static void mo_two_gemms(Handle& H, int precision, const double* U, int64_t kc, 
         CB(cublasDgemmStridedBatched_64(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, kc, NB, nao, &one, W1, kc, nao * kc, CBd,
                                         nao, 0, &zero, out, ldk * NA, ldk, NA));
     } else {
-        CU(mo_gemm_mixed(U, nao * kc, NA, nao, CAd, W1, C.stream));
-        CU(mo_gemm_mixed_batched(W1, kc, NB, nao, CBd, out, ldk, NA, C.stream));
+        // W1 (nao kc x NA) = U (rows (q,k), K = p) C_A; then per a: out_a (kc x NB) = W1_a (kc x nao) C_B
+        gemm_nt_split(nao * kc, NA, nao, 1.0, U, 1, nao * kc, CAd, nao, 1, 0.0, W1, nao * kc);
+        for (int64_t a = 0; a < NA; ++a)
+            gemm_nt_split(kc, NB, nao, 1.0, W1 + a * nao * kc, 1, kc, CBd, nao, 1, 0.0, out + a * ldk, ldk * NA);
     }
 }
 
@@ -1363,8 +1415,6 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
     if (NA <= 0 || NB <= 0) fail(GCI_ERR_ARG, "Invalid dimension of Rkab");
     if (ldca < nao || ldcb < nao) fail(GCI_ERR_ARG, "Invalid number of atomic orbitals in CA/CB");
     if (precision != GCI_PREC_FP64 && precision != GCI_PREC_MIXED) fail(GCI_ERR_ARG, "invalid precision mode");
-    if (precision == GCI_PREC_MIXED)
-        fail(GCI_ERR_UNSUPPORTED, "split-precision AO->MO GEMMs are not built (use GCI_PREC_FP64)");
     if (N == 0) return;
     // MO coefficient blocks on the device
     DVec<double> dCA, dCB, dOut, U, W1;
@@ -1449,7 +1499,6 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
             T.start(kMoGemm);
             mo_two_gemms(H, precision, U.p, jc, dCA.p, NA, dCB.p, NB, W1.p, Vab.p + J0, N);
             T.stop();
-            CU(cudaStreamSynchronize(s));
             k = k1;
         }
         T.start(kInvLGemm);
@@ -1458,6 +1507,7 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
         H.gemm_flops[kGemmInvL] += 2.0 * (double)N * N * NA * NB;
         T.stop();
     }
+    if (precision == GCI_PREC_MIXED) check_device_error(C, "split-precision AO->MO");
     if (!device_io) CU(cudaMemcpyAsync(rkab, dOut.p, sizeof(double) * N * NA * NB, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     T.flush();
@@ -1648,8 +1698,6 @@ static void coulomb_grad_impl(const gci_basis* basis, double omega, const double
 // chol_gammcor_Rkpq on the calling thread's context (stream).
 static void rkpq_run(Handle& H, const gci_basis* basis, int accuracy, double omega, int flags)
 {
-    if (flags & GCI_FLAG_MIXED_STEP1)
-        fail(GCI_ERR_UNSUPPORTED, "split-precision GEMMs for the pivot search are not built (FP64 only)");
     H.tau = accuracy_tau(accuracy);
     H.kappa = (omega > 0.0) ? 1.0 / (omega * omega) : 0.0;   // Cholesky_Gammcor.f90:412-421
     H.flags = flags;
@@ -1770,6 +1818,65 @@ int gci_copy_rkpq(const gci_handle* h, double* dst)
         if (!H.have_rkpq) fail(GCI_ERR_STATE, "Rkpq was not materialised (pass GCI_FLAG_MATERIALIZE_RKPQ)");
         const size_t n = (size_t)H.nvecs * H.msd * H.nsubsets;
         if (n) CU(cudaMemcpy(dst, H.rkpq.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+int gci_rkpq_columns(gci_handle* h, int64_t n, const int64_t* pq, double* out)
+{
+    if (!h || (n > 0 && (!pq || !out))) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    if (n < 0) { g_last_error = "n < 0"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        Context& C = ctx();
+        cudaStream_t s = C.stream;
+        Handle& H = h->h;
+        const PairTable& P = H.pt;
+        const HostBasis& b = H.hb;
+        const int64_t N = H.nvecs;
+        if (n == 0 || N == 0) return;
+        // FULL orbital-pair index -> (BASE pair, index within the pair's stored block)
+        std::vector<int64_t> owner(H.npq, -1);
+        for (int64_t s2 = 0; s2 < H.nsp; ++s2)
+            for (int i = 0; i < P.dim[H.bsp[s2]]; ++i) owner[H.fullloc[s2] + i] = s2;
+        std::vector<int> first(H.npq, -1);   // output column of each requested pair (first occurrence)
+        std::vector<int64_t> dup;            // (output column, its first occurrence) of repeated pairs
+        std::vector<char> used(H.nsp, 0);
+        for (int64_t c = 0; c < n; ++c) {
+            const int64_t f = pq[c] - 1;
+            if (f < 0 || f >= H.npq) fail(GCI_ERR_ARG, "orbital pair index out of range");
+            if (first[f] < 0) first[f] = (int)c;
+            else { dup.push_back(c); dup.push_back(first[f]); }
+            used[owner[f]] = 1;
+        }
+        PairMap rows;
+        rows.reset(P.n);
+        std::vector<int> ids;
+        for (int64_t s2 = 0; s2 < H.nsp; ++s2) {
+            if (!used[s2]) continue;
+            const int id = H.bsp[s2];
+            ids.push_back(id);
+            const int A = P.A[id], B = P.B[id], Na = b.nfunc[A], Nb = b.nfunc[B];
+            int* m = rows.add(id, Na * Nb);
+            for (int bb = 0; bb < Nb; ++bb)
+                for (int a = 0; a < Na; ++a) {
+                    const int64_t l = pair_local(a, bb, Na, A == B);
+                    m[a + Na * bb] = l < 0 ? -1 : first[H.fullloc[s2] + l];
+                }
+        }
+        rows.upload(s);
+        std::vector<int> pivids;
+        for (int64_t k = 0; k < H.npsp; ++k) pivids.push_back(H.bsp[H.psp[k]]);
+        DVec<double> W, R;
+        W.alloc((size_t)n * N);
+        CU(cudaMemsetAsync(W.p, 0, sizeof(double) * n * N, s));
+        run_eri(H, ids, pivids, kModeProduct, &rows, &H.pivmap, W.p, n);
+        // R(:, pq) = Inv_L W(pq, :)^T (TwoStepCholesky.f90:410-415 for these columns)
+        R.alloc((size_t)N * n);
+        gemm_nt(C.blas, N, n, N, 1.0, H.invl.p, N, W.p, n, 0.0, R.p, N);
+        for (size_t d = 0; d < dup.size(); d += 2)
+            CU(cudaMemcpyAsync(R.p + N * dup[d], R.p + N * dup[d + 1], sizeof(double) * N, cudaMemcpyDeviceToDevice,
+                               s));
+        CU(cudaMemcpyAsync(out, R.p, sizeof(double) * N * n, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
     });
 }
 
@@ -1968,6 +2075,23 @@ int gci_eri_pairs(const gci_basis* basis, double omega, double* out, int64_t ld)
         run_eri(H, all, all, kModeProduct, &m, &m, d.p, ld);
         CU(cudaMemcpyAsync(out, d.p, sizeof(double) * ld * npq, cudaMemcpyDeviceToHost, C.stream));
         CU(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int gci_dgemm_split(int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda, const double* B,
+                    int64_t ldb, double beta, double* Cm, int64_t ldc)
+{
+    if (m < 0 || n < 0 || k < 0 || lda < std::max<int64_t>(m, 1) || ldb < std::max<int64_t>(n, 1) ||
+        ldc < std::max<int64_t>(m, 1)) {
+        g_last_error = "invalid GEMM dimensions";
+        return GCI_ERR_ARG;
+    }
+    if ((m > 0 && n > 0 && k > 0) && (!A || !B || !Cm)) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        Context& C = ctx();
+        gemm_nt_split(m, n, k, alpha, A, 1, lda, B, 1, ldb, beta, Cm, ldc);
+        check_device_error(C, "gci_dgemm_split");
+        pool_trim();
     });
 }
 

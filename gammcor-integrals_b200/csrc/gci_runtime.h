@@ -29,6 +29,15 @@ cudaError_t hm_colvec_launch(const HmChunk* chunks, int nchunks, const ShellPair
                              const int* colfun, const double* tmat, const int* toff, const int* nfunc, double* vec,
                              cudaStream_t st);
 cudaError_t hm_launch(int L1, int L2, int nt, const HmArgs& a, cudaStream_t st);
+// Split-precision FP64 GEMM on the int8 tensor cores (ozaki_gemm.cu):
+// C = alpha A B^T + beta C with A(i, l) = A[i ars + l als], B(j, l) = B[j brs + l bls],
+// k <= ozaki_max_k(); `work` holds ozaki_workspace_bytes(m, n, k); `err` is set to 1
+// when a bounded wait of the GEMM kernel expires.
+size_t ozaki_workspace_bytes(int64_t m, int64_t n, int64_t k);
+int64_t ozaki_max_k();
+cudaError_t ozaki_dgemm_nt(int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t ars, int64_t als,
+                           const double* B, int64_t brs, int64_t bls, double beta, double* C, int64_t ldc,
+                           void* work, int* err, cudaStream_t st);
 cudaError_t boys_eval_launch(int m, int64_t n, const double* x, const double* table, double* out, cudaStream_t st);
 
 cudaError_t launch_segmax(const double* D, const int64_t* loc, const int* dim, int64_t n, double* out, cudaStream_t s);

@@ -7,7 +7,8 @@
  * This is the drop-in boundary for the reference's Gammcor interface
  * (modrzejewski/gammcor-integrals, src/gammcor-interface/Cholesky_Gammcor.f90).
  * A Fortran ISO_C_BINDING shim keeping the module Cholesky_Gammcor and the
- * type TCholeskyVecsOTF binds these entry points.
+ * type TCholeskyVecsOTF binds these entry points
+ * (gammcor-integrals_b200/fortran/cholesky_gammcor_gpu.f90).
  *
  * Conventions: arrays are column-major (Fortran order); indices passed in
  * arrays are 1-based exactly as in TAOBasis; integers are int64_t so that
@@ -42,10 +43,11 @@ extern "C" {
 #define GCI_FLAG_MATERIALIZE_RKPQ   1  /* store Rkpq on the device (otherwise Rkab is built from V(pq,J) directly) */
 #define GCI_FLAG_PIVOT_DECODE_STORAGE 2 /* decode diagonal-shell-pair pivots in storage order (the reference decodes
                                           them with chol2_pq2p_ge_q, TwoStepCholesky_Step2.f90:422-466) */
-#define GCI_FLAG_MIXED_STEP1        4  /* split-precision GEMMs in the pivot search: not built, rejected with
-                                          GCI_ERR_UNSUPPORTED */
+#define GCI_FLAG_MIXED_STEP1        4  /* M - L L^T of the pivot search (chol2_SubtractR) as a split-precision
+                                          GEMM on the int8 tensor cores (gci_dgemm_split) */
 
-/* Precision of the AO->MO GEMMs (GCI_PREC_MIXED, split precision, is not built: GCI_ERR_UNSUPPORTED) */
+/* Precision of the AO->MO GEMMs: FP64 (cuBLAS DGEMM) or split precision on the int8
+ * tensor cores (gci_dgemm_split) */
 #define GCI_PREC_FP64   0
 #define GCI_PREC_MIXED  1
 
@@ -110,6 +112,13 @@ int gci_copy_chol2data(const gci_handle *h, int64_t *shellpairs, int64_t *shellp
                        int64_t *subsetdim, int64_t *subsetbounds, int64_t *pivots, int64_t *pivotshellpairs,
                        int64_t *pivotshellpairloc, int64_t *pivotshellpairdim, int64_t *pivotorbpairs,
                        double *inv_l);
+
+/* Columns R(:, pq) of the Cholesky vectors for n orbital pairs (FULL-storage indices,
+ * 1-based, repeats allowed) without materialising Rkpq: the full-dimension integrals of
+ * those pairs against the pivot columns (chol2_Vabrs, TwoStepCholesky_Step2.f90:242-419,
+ * restricted to their shell pairs) times Inv_L (chol2_FullDimVectors_Batch,
+ * TwoStepCholesky.f90:378-416).  out: NVecs x n, column-major, host memory. */
+int gci_rkpq_columns(gci_handle *h, int64_t n, const int64_t *pq, double *out);
 
 /* Pivot sequence of step 1 (FULL-storage orbital-pair indices, 1-based, selection order)
  * and the residual diagonal at each selection.  Either pointer may be NULL. */
@@ -182,6 +191,15 @@ int gci_eri_pairs(const gci_basis *basis, double omega, double *out, int64_t ld)
  * queries; returns the variant in use (>= 0) or GCI_ERR_ARG.  The choice is
  * process-wide. */
 int gci_eri_variant(int tb, int tk, int variant);
+
+/* Split-precision FP64 GEMM on the int8 tensor cores (no counterpart in the reference; the
+ * split-precision form of its dgemm calls, real_linalg.f90:1331-1361): C = alpha A B^T + beta C
+ * with A (m x k), B (n x k), C (m x n) column-major DEVICE pointers on the library's stream.
+ * Each row of A and B is scaled by a power of two and cut into seven 8-bit slices (Ozaki
+ * splitting); the 34 slice products with s + t <= 9 run as tcgen05 int8 MMAs with exact int32
+ * accumulation and are recombined in FP64.  Error ~1e-12 of max|A_i| max|B_j| for k = 16k. */
+int gci_dgemm_split(int64_t m, int64_t n, int64_t k, double alpha, const double *A, int64_t lda,
+                    const double *B, int64_t ldb, double beta, double *C, int64_t ldc);
 
 /* Hermite-matrix ERI kernels (default on).  For spherical bases the
  * product-mode stages (step-1 pivot columns, the pivot block, the

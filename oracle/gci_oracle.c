@@ -1675,3 +1675,45 @@ int orc_coulomb_energy_grad(const orc_basis *b, const int *shell_atom, int natom
     *energy = e;
     return 0;
 }
+
+/* Timing sample of the reference algorithm (test and benchmark
+ * infrastructure): n shell quartets (A, B, C, D per quartet, 0-based)
+ * evaluated by orc_eri_quartet over `nthreads` OpenMP threads; the integrals
+ * are folded into a checksum so that the work is not discarded. */
+double orc_eri_quartets_batch(const orc_basis *b, int64_t n, const int *quads, double kappa, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+    if (orc_boys_init(4 * ORC_MAXL) != 0) return 0.0;
+    double sum = 0.0;
+#pragma omp parallel reduction(+ : sum)
+    {
+        double *V = (double *)malloc(sizeof(double) * 10000);
+#pragma omp for schedule(dynamic)
+        for (int64_t q = 0; q < n; ++q) {
+            const int *s = quads + 4 * q;
+            if (orc_eri_quartet(b, s[0], s[1], s[2], s[3], kappa, V) == 0) {
+                const int tot = nfunc(b, s[0]) * nfunc(b, s[1]) * nfunc(b, s[2]) * nfunc(b, s[3]);
+                for (int i = 0; i < tot; ++i) sum += V[i];
+            }
+        }
+        free(V);
+    }
+    return sum;
+}
+
+/* Exported forms of the Hermite recursions for the fixture tests: R_tuv for
+ * t+u+v <= n in level-major order (herm_idx), and the
+ * single-centre E^{e}_t, [emax+1][emax+1]. */
+void orc_rtuv(int n, const double *F, double alpha, double X, double Y, double Z, double *R)
+{
+    rtuv(n, F, alpha, X, Y, Z, R);
+}
+
+void orc_et_coeffs(int emax, double p, double X, double *E)
+{
+    et_coeffs(emax, p, X, E);
+}

@@ -56,6 +56,13 @@ int orc_eri_quartet(const orc_basis *b, int A, int B, int C, int D, double kappa
  * 0 the reference's W-matrix + HRR route (auto2e), which loses all digits on
  * (ff|ff)-type quartets of shells that mix tight and diffuse primitives. */
 void orc_set_eri_scheme(int scheme);
+/* Hermite recursions (fixture tests): R_tuv, t+u+v <= n, level-major order;
+ * single-centre E^{e}_t as [emax+1][emax+1] (e major). */
+void orc_rtuv(int n, const double *F, double alpha, double X, double Y, double Z, double *R);
+void orc_et_coeffs(int emax, double p, double X, double *E);
+/* Timing sample: n quartets (4 shell indices each) over nthreads OpenMP
+ * threads; returns the sum of all integrals. */
+double orc_eri_quartets_batch(const orc_basis *b, int64_t n, const int *quads, double kappa, int nthreads);
 
 /* ---------------- two-step Cholesky (TwoStepCholesky*.f90) ---------------- */
 typedef struct {

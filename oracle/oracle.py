@@ -74,6 +74,10 @@ def lib():
                                           C.c_int, _pl, _i64, C.c_int, C.POINTER(_Chol)]
         L.orc_stats.argtypes = [_pd, C.c_int]
         L.orc_stats_reset.argtypes = []
+        L.orc_rtuv.argtypes = [C.c_int, _pd, C.c_double, C.c_double, C.c_double, C.c_double, _pd]
+        L.orc_et_coeffs.argtypes = [C.c_int, C.c_double, C.c_double, _pd]
+        L.orc_eri_quartets_batch.argtypes = [C.POINTER(_Basis), _i64, _pi, C.c_double, C.c_int]
+        L.orc_eri_quartets_batch.restype = C.c_double
         L.orc_set_eri_scheme.argtypes = [C.c_int]
         L.orc_set_eri_scheme.restype = None
         L.orc_chol_free.argtypes = [C.POINTER(_Chol)]
@@ -193,6 +197,34 @@ def eri_quartet(b: OracleBasis, A, B, Cc, D, kappa=0.0) -> np.ndarray:
     if rc != 0:
         raise RuntimeError(f"orc_eri_quartet failed ({rc})")
     return out.reshape(nf[::-1]).transpose(3, 2, 1, 0)   # [a, b, c, d]
+
+
+def herm_idx(t: int, u: int, v: int) -> int:
+    """Level-major position of the Hermite index (t, u, v) (all of level < t+u+v first)."""
+    n = t + u + v
+    return n * (n + 1) * (n + 2) // 6 + (u + v) * (u + v + 1) // 2 + v
+
+
+def rtuv(n: int, F, alpha: float, X: float, Y: float, Z: float) -> np.ndarray:
+    """R_tuv for t+u+v <= n (level-major order) from F_0..F_n."""
+    Fv = np.ascontiguousarray(F, dtype=np.float64)
+    out = np.zeros((n + 1) * (n + 2) * (n + 3) // 6)
+    lib().orc_rtuv(n, _p(Fv), alpha, X, Y, Z, _p(out))
+    return out
+
+
+def et_coeffs(emax: int, p: float, X: float) -> np.ndarray:
+    """Single-centre Hermite coefficients E^{e}_t, shape (emax+1, emax+1)."""
+    out = np.zeros((emax + 1) * (emax + 1))
+    lib().orc_et_coeffs(emax, p, X, _p(out))
+    return out.reshape(emax + 1, emax + 1)
+
+
+def eri_quartets_batch(b: OracleBasis, quads, kappa=0.0, nthreads=0) -> float:
+    """Evaluate the shell quartets `quads` (n x 4, 0-based) over nthreads OpenMP
+    threads and return the sum of the integrals (timing samples)."""
+    q = np.ascontiguousarray(np.asarray(quads, dtype=np.int32).reshape(-1, 4))
+    return float(lib().orc_eri_quartets_batch(C.byref(b.cstruct()), q.shape[0], _p(q, _pi), kappa, nthreads))
 
 
 def eri_full(b: OracleBasis, kappa=0.0, nthreads=0) -> np.ndarray:

@@ -195,3 +195,26 @@ def test_orbital_ordering_round_trip(ordering):
     Y = ai.auto2e_interface_AngFuncTransf(X, True, False, tb, ordering)
     Z = ai.auto2e_interface_AngFuncTransf(Y, False, False, tb, ordering)
     np.testing.assert_array_equal(X, Z)
+
+
+def test_rtuv_matches_reference_generator():
+    """The oracle's R_tuv recursion against the statements the reference's
+    generator emits for auto2e_Rtuv_n / auto2e_RtuvK_k (Auto2e.py:80-119,1027-1066),
+    evaluated at seeded inputs (tests/golden/hermite_recurrences.json), n = 0..12."""
+    gold = json.loads((GOLD / "hermite_recurrences.json").read_text())
+    for c in gold["rtuv"]:
+        R = O.rtuv(c["n"], c["F"], c["alpha"], c["X"], c["Y"], c["Z"])
+        ref = np.array([r[3] for r in c["R"]])
+        got = np.array([R[O.herm_idx(t, u, v)] for t, u, v, _ in c["R"]])
+        assert len(got) == len(R)
+        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * np.max(np.abs(ref)))
+
+
+def test_et_coeffs_match_reference_generator():
+    """The oracle's single-centre Hermite coefficients against the statements of
+    auto2e_EtCoeffs_L (Auto2e.py:997-1025), L = 0..12."""
+    gold = json.loads((GOLD / "hermite_recurrences.json").read_text())
+    for c in gold["et"]:
+        E = O.et_coeffs(c["L"], c["p"], c["X"])
+        for l, t, v in c["E"]:
+            assert abs(E[l, t] - v) <= 1e-12 * max(1.0, abs(v)), (c["L"], l, t, E[l, t], v)

@@ -1,0 +1,62 @@
+"""GPU parity at the c2 configuration (40 atoms, NAO = 1200, tau = 1e-6) on a
+seeded sample: the Cholesky vectors of the orbital pairs of a few BASE shell
+pairs of every pair type (gci_rkpq_columns, no materialised Rkpq) reconstruct
+the exact integrals (pq|rs) of the oracle within the decomposition's own
+bound tau (|V - L L^T| <= sqrt(D_pq D_rs) <= tau at convergence,
+TwoStepCholesky_Step1.f90:884-1103).  This checks the pivot search, the pivot
+block, Inv_L and the full-dimension integrals of the real configuration,
+which the oracle cannot decompose in test time."""
+import numpy as np
+import pytest
+
+from gammcor_integrals_b200 import _capi, molecules
+from gammcor_integrals_b200 import cholesky_gammcor as cg
+from helpers import both
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _stored_functions(same: bool, na: int, nb: int):
+    """(a, b) of each orbital pair of a shell pair in FULL storage order
+    (chol2_write_Vdiag, TwoStepCholesky_Step1.f90:175-199)."""
+    return [(a, b) for b in range(nb) for a in range(b if same else 0, na)]
+
+
+def test_c2_sampled_reconstruction(gpu_lib):
+    mol = molecules.config("c2")
+    tb, ob = both(mol)
+    res = cg.chol_gammcor_Rkpq(tb, cg.CHOL_ACCURACY_TIGHT, materialize=False)
+    d = res.Chol2Data
+    sp = d.ShellPairs.T - 1
+    loc = d.ShellPairLoc[0] - 1
+    nf = [2 * int(ob.L[s]) + 1 for s in range(len(ob.L))]
+    by_type = {}
+    for s in range(d.NShellPairs):
+        la, lb = int(ob.L[sp[s, 0]]), int(ob.L[sp[s, 1]])
+        by_type.setdefault((max(la, lb), min(la, lb)), []).append(s)
+    rng = np.random.default_rng(8)
+    chosen = []
+    for key in sorted(by_type):
+        pairs = by_type[key]
+        chosen.extend(int(x) for x in rng.choice(pairs, size=min(3, len(pairs)), replace=False))
+    blocks, pq = [], []
+    for s in chosen:
+        A, B = int(sp[s, 0]), int(sp[s, 1])
+        fun = _stored_functions(A == B, nf[A], nf[B])
+        blocks.append((A, B, len(pq), fun))
+        pq.extend(int(loc[s]) + 1 + k for k in range(len(fun)))
+    pq = np.array(pq, dtype=np.int64)
+    R = np.zeros((d.NVecs, len(pq)), order="F")
+    _capi.check(gpu_lib.gci_rkpq_columns(res.handle.ptr, len(pq), _capi.ptr(pq, _capi._pl), _capi.ptr(R)))
+    rec = R.T @ R
+    exact = np.zeros_like(rec)
+    for i, (A, B, o1, f1) in enumerate(blocks):
+        for (C_, D_, o2, f2) in blocks[i:]:
+            G = O.eri_quartet(ob, A, B, C_, D_)
+            blk = np.array([[G[a, b, c, e] for (c, e) in f2] for (a, b) in f1])
+            exact[o1:o1 + len(f1), o2:o2 + len(f2)] = blk
+            exact[o2:o2 + len(f2), o1:o1 + len(f1)] = blk.T
+    err = np.max(np.abs(exact - rec))
+    assert len(blocks) >= 20 and len(pq) > 300
+    assert err <= 1.001 * mol.tau, err

@@ -52,24 +52,29 @@ def _vdiag_order_pairs(ob):
 
 
 class _Variants:
-    """Force one ERI kernel variant on every class that has it; restore on exit."""
+    """Force one kernel family on the product stages: "hermite" (the Hermite-matrix
+    kernels) or a class-kernel variant 0..3 on every class that has it (-1 keeps
+    the current variants); restore everything on exit."""
 
     def __init__(self, lib, variant):
-        self.lib, self.variant, self.saved = lib, variant, {}
+        self.lib, self.variant, self.saved, self.hm = lib, variant, {}, None
 
     def __enter__(self):
-        for tb in range(10):
-            for tk in range(tb + 1):
-                self.saved[(tb, tk)] = self.lib.gci_eri_variant(tb, tk, -1)
-                self.lib.gci_eri_variant(tb, tk, self.variant)   # GCI_ERR_ARG where not built
+        self.hm = self.lib.gci_eri_hm(1 if self.variant == "hermite" else 0)
+        if self.variant != "hermite":
+            for tb in range(10):
+                for tk in range(tb + 1):
+                    self.saved[(tb, tk)] = self.lib.gci_eri_variant(tb, tk, -1)
+                    self.lib.gci_eri_variant(tb, tk, self.variant)   # GCI_ERR_ARG where not built
         return self
 
     def __exit__(self, *exc):
         for (tb, tk), v in self.saved.items():
             self.lib.gci_eri_variant(tb, tk, v)
+        self.lib.gci_eri_hm(self.hm)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", ["hermite", 0, 1, 2, 3])
 @pytest.mark.parametrize("recipe,seed,natoms", [(molecules.RECIPE_C1, 11, 3), (molecules.RECIPE_C2, 12, 2)])
 def test_eri_blocks_all_classes(gpu_lib, recipe, seed, natoms, variant):
     mol = molecules.small_molecule(seed, natoms=natoms, recipe=recipe, nprim=(3, 4))
@@ -215,3 +220,32 @@ def test_rkab_direct_and_materialised(gpu_lib):
     np.testing.assert_array_equal(res2.pivot_order, res.pivot_order)
     got2 = cg.chol_gammcor_Rkab(Cm, a0, a1, Cm, b0, b1, 1, res2, tb)
     assert np.max(np.abs(got2 - ref)) < 1e-8
+
+
+def test_c1_job_parity(gpu_lib):
+    """The c1 benchmark configuration end to end (10 atoms, NAO = 140, tau = 1e-6,
+    MO 20 occupied x 60 virtual of the seeded C) against the oracle: the pivot
+    sequence at shell-pair level with residual diagonals up to the first symmetry
+    tie; on the GPU's pivot set the vectors through R^T R, V_JJ's inverse factor
+    Inv_L, and Rkab with the MO integrals it reconstructs, through the stored and
+    the direct AO->MO paths, all to 1e-8 absolute."""
+    mol = molecules.config("c1")
+    tb, ob, res, ch = _run_both(mol)
+    _assert_equivalent_sequences(res, ch)
+    ch2 = _assert_step2_parity(tb, ob, res, mol)
+    # Inv_L elementwise, relative to its largest entry (~1/sqrt(tau)): the pivot block's
+    # condition number (max diagonal / tau ~ 1e7) times FP64 rounding; measured 2.4e-9
+    rel = np.max(np.abs(res.Chol2Data.Inv_L - ch2.inv_l)) / np.max(np.abs(ch2.inv_l))
+    assert rel < 1e-7, rel
+    nocc, nvirt, seed = molecules.MO_SPLIT["c1"]
+    Cm = molecules.mo_coefficients(tb.NAO, seed)
+    ref = O.mo_transf(ch2, ob, Cm, 0, nocc - 1, Cm, nocc, nocc + nvirt - 1)
+    got = cg.chol_gammcor_Rkab(Cm, 1, nocc, Cm, nocc + 1, nocc + nvirt, 1024, res, tb)
+    assert np.max(np.abs(got - ref)) < 1e-8
+    assert np.max(np.abs(got.T @ got - ref.T @ ref)) < 1e-8
+    res2 = cg.chol_gammcor_Rkpq(tb, cg.CHOL_ACCURACY_TIGHT, materialize=False)
+    np.testing.assert_array_equal(res2.pivot_order, res.pivot_order)
+    got2 = cg.chol_gammcor_Rkab(Cm, 1, nocc, Cm, nocc + 1, nocc + nvirt, 1024, res2, tb)
+    assert np.max(np.abs(got2 - ref)) < 1e-8
+    O.free(ch)
+    O.free(ch2)

@@ -2,9 +2,10 @@
 
 It must give the same ERI matrix as gci_eri_pairs (within the 1e-10 x max
 tolerance of the ERI parity tests) on consecutive calls that reuse its one
-fixed scratch, reject a basis whose tables exceed that scratch, and work as
-the first libgci call of a fresh process.  Collected last (file name) so that
-it also runs after every other test has used the library.
+fixed scratch, leave the device's free memory unchanged while doing so, and
+reject a basis whose tables exceed that scratch.  Collected last (file name)
+so that a run that stops at the first failure has run every other test
+first; it passes alone in a fresh process as well as after the others.
 """
 import ctypes as C
 
@@ -20,14 +21,23 @@ def _npq(tb):
     return tb.NAO * (tb.NAO + 1) // 2
 
 
-def _noalloc(tb, ld, stream):
+def _output(tb, ld, stream):
+    """NaN-filled column-major ld x NPQ output, written on `stream` (the stream the
+    library call will use), so that the fill is ordered before the call."""
     import torch
-    out = torch.full((_npq(tb), ld), float("nan"), dtype=torch.float64, device="cuda")   # column-major ld x NPQ
-    s = tb.c_struct()
     with torch.cuda.stream(stream):
-        rc = _capi.lib().gci_eri_pairs_noalloc(C.byref(s), 0.0, C.c_void_p(out.data_ptr()), ld,
-                                               C.c_void_p(stream.cuda_stream))
-    return rc, out
+        return torch.full((_npq(tb), ld), float("nan"), dtype=torch.float64, device="cuda")
+
+
+def _call(tb, ld, out, stream):
+    s = tb.c_struct()
+    return _capi.lib().gci_eri_pairs_noalloc(C.byref(s), 0.0, C.c_void_p(out.data_ptr()), ld,
+                                             C.c_void_p(stream.cuda_stream))
+
+
+def _noalloc(tb, ld, stream):
+    out = _output(tb, ld, stream)
+    return _call(tb, ld, out, stream), out
 
 
 def _reference(tb, ld):
@@ -53,12 +63,25 @@ def test_noalloc_matches_eri_pairs_on_consecutive_calls():
     tb_b = gbasis.from_molecule(molecules.small_molecule(12, natoms=2, recipe=molecules.RECIPE_C2, nprim=(3, 4)))
     ld_a, ld_b = _npq(tb_a) + 3, _npq(tb_b)
     stream = torch.cuda.Stream()
-    rc_a, got_a = _noalloc(tb_a, ld_a, stream)      # first library call of a fresh process
-    rc_b, got_b = _noalloc(tb_b, ld_b, stream)
+    # one call per basis first: they load the library's device code for every
+    # class involved (lazily loaded kernels take device memory on first use),
+    # and the first looks up the scratch's device address
+    for tb, ld in ((tb_a, ld_a), (tb_b, ld_b)):
+        rc0, _ = _noalloc(tb, ld, stream)
+        _capi.check(rc0)
+    out_a = _output(tb_a, ld_a, stream)
+    out_b = _output(tb_b, ld_b, stream)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    rc_a = _call(tb_a, ld_a, out_a, stream)
+    rc_b = _call(tb_b, ld_b, out_b, stream)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
     _capi.check(rc_a)
     _capi.check(rc_b)
-    _check(got_a, _reference(tb_a, ld_a))
-    _check(got_b, _reference(tb_b, ld_b))
+    assert free1 == free0, f"device free memory changed by {free0 - free1} bytes across the two calls"
+    _check(out_a, _reference(tb_a, ld_a))
+    _check(out_b, _reference(tb_b, ld_b))
 
 
 def test_noalloc_rejects_basis_beyond_scratch():
