@@ -590,9 +590,9 @@ def main():
         _capi.check(L.gci_stats(h, _capi.ptr(st), st.size))
         tm = np.zeros(13)
         _capi.check(L.gci_timings(h, _capi.ptr(tm), 13))
-        hs = np.zeros(7 * 7 * 3 * 3)
+        hs = np.zeros(7 * 7 * 7 * 3)
         _capi.check(L.gci_eri_hm_stats(h, _capi.ptr(hs), hs.size))
-        state["hm"] = hs.reshape(7, 7, 3, 3)
+        state["hm"] = hs.reshape(7, 7, 7, 3)
         L.gci_free(h)
         return st, tm
 
@@ -629,7 +629,7 @@ def main():
         hs = state["hm"]
         tot = hs[..., 1].sum()
         rows = sorted(((hs[a, b, c, 1], a, b, c + 1, hs[a, b, c, 0], hs[a, b, c, 2])
-                       for a in range(7) for b in range(7) for c in range(3) if hs[a, b, c, 0] > 0), reverse=True)
+                       for a in range(7) for b in range(7) for c in range(7) if hs[a, b, c, 0] > 0), reverse=True)
         print(f"# Hermite-matrix classes: {tot:.2f} s, {hs[..., 2].sum() / 1e12:.1f} TFLOP issued", file=sys.stderr)
         for t, a, b, c, n, f in rows:
             print(f"#  L1={a} L2={b} NT={c}  launches {int(n):5d}  {t:8.3f} s  {100 * t / max(tot, 1e-30):5.1f}%  "

@@ -381,13 +381,18 @@ static cudaError_t launch_hm(const HmArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// tab[L1][L2][NT - 1] for L2 = 0 .. kMaxPairL
+// tab[L1][L2][NT - 1] for L2 = 0 .. kMaxPairL and NT = 1 .. hm_max_nt(L1)
+template <int L1, int L2, int NT = 1>
+static void register_hm_nt(HmLaunchFn (*tab)[kMaxPairL + 1][kHmMaxNT])
+{
+    tab[L1][L2][NT - 1] = &launch_hm<L1, L2, NT>;
+    if constexpr (NT < hm_max_nt(L1)) register_hm_nt<L1, L2, NT + 1>(tab);
+}
+
 template <int L1, int L2 = 0>
 static void register_hm_row(HmLaunchFn (*tab)[kMaxPairL + 1][kHmMaxNT])
 {
-    tab[L1][L2][0] = &launch_hm<L1, L2, 1>;
-    tab[L1][L2][1] = &launch_hm<L1, L2, 2>;
-    tab[L1][L2][2] = &launch_hm<L1, L2, 3>;
+    register_hm_nt<L1, L2>(tab);
     if constexpr (L2 < kMaxPairL) register_hm_row<L1, L2 + 1>(tab);
 }
 

@@ -163,7 +163,8 @@ cudaError_t hm_launch(int L1, int L2, int nt, const HmArgs& a, cudaStream_t st)
 {
     static std::once_flag once;
     std::call_once(once, hm_register);
-    if (L1 < 0 || L2 < 0 || L1 > kMaxPairL || L2 > kMaxPairL || nt < 1 || nt > kHmMaxNT) return cudaErrorInvalidValue;
+    if (L1 < 0 || L2 < 0 || L1 > kMaxPairL || L2 > kMaxPairL || nt < 1 || nt > hm_max_nt(L1) || !g_hm[L1][L2][nt - 1])
+        return cudaErrorInvalidValue;
     cudaError_t e = g_hm[L1][L2][nt - 1](a, st);
     count_launch();
     return e;

@@ -577,40 +577,48 @@ static void run_eri_hm(Handle& H, const std::vector<int>& gb, const std::vector<
     Context& C = ctx();
     const PairTable& P = H.pt;
     hm_ensure_rows(H, gb);
-    // column chunks of at most 8 kHmMaxNT columns, grouped by (column type, tiles)
+    // column chunks, one set per chunk width in use: rows of level L1 take chunks of at
+    // most 8 hm_max_nt(L1) columns; within a set, grouped by (column type, tiles)
+    bool width_used[kHmMaxNT + 1] = {};
+    for (int tb = 0; tb < kNumPairTypes; ++tb)
+        if (sb[tb + 1] > sb[tb]) width_used[hm_max_nt(type_lsum(tb))] = true;
     std::vector<HmChunk> chunks;
     std::vector<int> colfun, colout;
-    std::vector<std::vector<int>> group((size_t)kNumPairTypes * kHmMaxNT);
+    auto gidx = [](int w, int tk, int nt) { return ((size_t)w * kNumPairTypes + tk) * kHmMaxNT + nt - 1; };
+    std::vector<std::vector<int>> group((size_t)(kHmMaxNT + 1) * kNumPairTypes * kHmMaxNT);
     int64_t voff = 0;
     std::vector<int> fl, ol;
-    for (int tk = 0; tk < kNumPairTypes; ++tk)
-        for (int64_t q = sk[tk]; q < sk[tk + 1]; ++q) {
-            const int id = gk[q];
-            const int nab = P.nab[id];
-            const int* m = cols->map.data() + cols->off[id];
-            fl.clear(); ol.clear();
-            for (int f = 0; f < nab; ++f)
-                if (m[f] >= 0) { fl.push_back(f); ol.push_back(m[f]); }
-            const int n = (int)fl.size();
-            if (n == 0) continue;
-            const int nch = (n + 8 * kHmMaxNT - 1) / (8 * kHmMaxNT);
-            const ShellPairDev& d = P.h[id];
-            const int L = d.l1 + d.l2;
-            for (int c = 0, beg = 0; c < nch; ++c) {
-                const int cnt = n / nch + (c < n % nch ? 1 : 0);
-                HmChunk ch{};
-                ch.pair = id;
-                ch.ncol = cnt;
-                ch.nt = (cnt + 7) / 8;
-                ch.vec_off = voff;
-                ch.col_off = (int64_t)colfun.size();
-                voff += (int64_t)d.npp * hm_col_stride(L, ch.nt);
-                for (int j = beg; j < beg + cnt; ++j) { colfun.push_back(fl[j]); colout.push_back(ol[j]); }
-                beg += cnt;
-                group[(size_t)tk * kHmMaxNT + ch.nt - 1].push_back((int)chunks.size());
-                chunks.push_back(ch);
+    for (int w = 1; w <= kHmMaxNT; ++w) {
+        if (!width_used[w]) continue;
+        for (int tk = 0; tk < kNumPairTypes; ++tk)
+            for (int64_t q = sk[tk]; q < sk[tk + 1]; ++q) {
+                const int id = gk[q];
+                const int nab = P.nab[id];
+                const int* m = cols->map.data() + cols->off[id];
+                fl.clear(); ol.clear();
+                for (int f = 0; f < nab; ++f)
+                    if (m[f] >= 0) { fl.push_back(f); ol.push_back(m[f]); }
+                const int n = (int)fl.size();
+                if (n == 0) continue;
+                const int nch = (n + 8 * w - 1) / (8 * w);
+                const ShellPairDev& d = P.h[id];
+                const int L = d.l1 + d.l2;
+                for (int c = 0, beg = 0; c < nch; ++c) {
+                    const int cnt = n / nch + (c < n % nch ? 1 : 0);
+                    HmChunk ch{};
+                    ch.pair = id;
+                    ch.ncol = cnt;
+                    ch.nt = (cnt + 7) / 8;
+                    ch.vec_off = voff;
+                    ch.col_off = (int64_t)colfun.size();
+                    voff += (int64_t)d.npp * hm_col_stride(L, ch.nt);
+                    for (int j = beg; j < beg + cnt; ++j) { colfun.push_back(fl[j]); colout.push_back(ol[j]); }
+                    beg += cnt;
+                    group[gidx(w, tk, ch.nt)].push_back((int)chunks.size());
+                    chunks.push_back(ch);
+                }
             }
-        }
+    }
     if (chunks.empty()) return;
     std::vector<int> order;
     std::vector<int64_t> gstart(group.size() + 1, 0);
@@ -648,8 +656,11 @@ static void run_eri_hm(Handle& H, const std::vector<int>& gb, const std::vector<
     // one task counter per launch
     int64_t nlaunch = 0;
     for (int tb = 0; tb < kNumPairTypes; ++tb)
-        if (sb[tb + 1] > sb[tb])
-            for (size_t g = 0; g < group.size(); ++g) nlaunch += gstart[g + 1] > gstart[g] ? 1 : 0;
+        if (sb[tb + 1] > sb[tb]) {
+            const int w = hm_max_nt(type_lsum(tb));
+            for (int tk = 0; tk < kNumPairTypes; ++tk)
+                for (int nt = 1; nt <= w; ++nt) nlaunch += gstart[gidx(w, tk, nt) + 1] > gstart[gidx(w, tk, nt)] ? 1 : 0;
+        }
     if (nlaunch == 0) return;
     H.hm_counters.ensure((size_t)nlaunch);
     CU(cudaMemsetAsync(H.hm_counters.p, 0, sizeof(unsigned long long) * nlaunch, C.stream));
@@ -676,9 +687,10 @@ static void run_eri_hm(Handle& H, const std::vector<int>& gb, const std::vector<
             npb += P.h[id].npp;
             rowt += (double)P.h[id].npp * ((P.nab[id] + 7) / 8);
         }
+        const int w = hm_max_nt(L1);
         for (int tk = 0; tk < kNumPairTypes; ++tk)
-            for (int nt = 1; nt <= kHmMaxNT; ++nt) {
-                const size_t g = (size_t)tk * kHmMaxNT + nt - 1;
+            for (int nt = 1; nt <= w; ++nt) {
+                const size_t g = gidx(w, tk, nt);
                 const int64_t nc = gstart[g + 1] - gstart[g];
                 if (nc == 0) continue;
                 const int L2 = type_lsum(tk);
@@ -742,6 +754,17 @@ static void run_eri(Handle& H, const std::vector<int>& bra, const std::vector<in
     };
     group(bra, gb, sb);
     if (mode != kModeDiagonal) group(ket, gk, sk);
+    if (hm) {
+        // longest tasks first: within each pair type, pairs with more primitive
+        // pairs come first, so that a launch's last tasks are its shortest
+        auto by_work = [&](std::vector<int>& g, const std::vector<int64_t>& seg) {
+            for (int t = 0; t < kNumPairTypes; ++t)
+                std::stable_sort(g.begin() + seg[t], g.begin() + seg[t + 1],
+                                 [&](int x, int y) { return P.h[x].npp > P.h[y].npp; });
+        };
+        by_work(gb, sb);
+        by_work(gk, sk);
+    }
     H.d_bra.upload(gb, C.stream);
     if (mode != kModeDiagonal) H.d_ket.upload(gk, C.stream);
     EriArgs a{};

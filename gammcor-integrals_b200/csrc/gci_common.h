@@ -163,7 +163,10 @@ GCI_HD constexpr int hm_mto(int L) { return (hm_max_nf(L) + 7) / 8; } // 8-row t
 GCI_HD constexpr int hm_row_stride(int L) { return hm_mto(L) * 2 * hm_mt(L) * 32; }
 // doubles of one column primitive pair's vectors in a chunk of NT column tiles: [KT][NT][32]
 GCI_HD constexpr int hm_col_stride(int L, int nt) { return hm_kt(L) * nt * 32; }
-constexpr int kHmMaxNT = 3;   // column tiles per task (24 columns)
+constexpr int kHmMaxNT = 7;   // column tiles per task, at most (56 columns)
+// Column tiles per task for rows of Hermite level L1: the 8x8 accumulator tiles of
+// X (ceil(H1/8) x NT) stay within ~66 registers.
+GCI_HD constexpr int hm_max_nt(int L1) { return L1 <= 3 ? 7 : (L1 == 4 ? 4 : 3); }
 
 // A group of at most 8 * NT requested columns of one column pair.
 struct HmChunk {

@@ -215,9 +215,9 @@ int gci_eri_hm(int enable);
 
 /* Work of the Hermite-matrix kernels of a decomposition (and its gci_rkab
  * calls): for every row level L1 (0..6), column level L2 (0..6) and column
- * tile count (1..3), in that order: launches, device seconds (measured only
- * with gci_eri_hm(2)) and tensor-core flops issued (padding included);
- * 7 x 7 x 3 x 3 values. */
+ * tile count (1..7, at most 7 for L1 <= 3, 4 for L1 = 4, 3 above), in that
+ * order: launches, device seconds (measured only with gci_eri_hm(2)) and
+ * tensor-core flops issued (padding included); 7 x 7 x 7 x 3 values. */
 int gci_eri_hm_stats(const gci_handle *h, double *out, int n);
 
 /* Autotuner: times every variant of every class that occurs in `basis` on a
