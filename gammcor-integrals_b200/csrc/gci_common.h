@@ -165,8 +165,8 @@ GCI_HD constexpr int hm_row_stride(int L) { return hm_mto(L) * 2 * hm_mt(L) * 32
 GCI_HD constexpr int hm_col_stride(int L, int nt) { return hm_kt(L) * nt * 32; }
 constexpr int kHmMaxNT = 7;   // column tiles per task, at most (56 columns)
 // Column tiles per task for rows of Hermite level L1: the 8x8 accumulator tiles of
-// X (ceil(H1/8) x NT) stay within ~66 registers.
-GCI_HD constexpr int hm_max_nt(int L1) { return L1 <= 3 ? 7 : (L1 == 4 ? 4 : 3); }
+// X (ceil(H1/8) x NT) stay at about 30 or fewer (two doubles per lane each).
+GCI_HD constexpr int hm_max_nt(int L1) { return L1 <= 3 ? 7 : (L1 == 4 ? 5 : (L1 == 5 ? 4 : 3)); }
 
 // A group of at most 8 * NT requested columns of one column pair.
 struct HmChunk {
