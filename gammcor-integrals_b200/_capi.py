@@ -26,7 +26,8 @@ GCI_NOALLOC_SCRATCH_BYTES = 16 << 20
 EXPORTS = ("gci_init", "gci_rkpq", "gci_query", "gci_copy_rkpq", "gci_copy_chol2data", "gci_pivot_order",
            "gci_rkab", "gci_timings", "gci_free", "gci_last_error", "gci_boys", "gci_spher_coeffs",
            "gci_normalize_basis", "gci_eri_pairs", "gci_rkab_device", "gci_stats", "gci_get_stream",
-           "gci_kernel_launches", "gci_eri_pairs_noalloc", "gci_eri_variant", "gci_eri_hm", "gci_eri_hm_stats", "gci_rkpq_columns", "gci_dgemm_split", "gci_autotune_eri",
+           "gci_kernel_launches", "gci_eri_pairs_noalloc", "gci_eri_variant", "gci_eri_hm", "gci_eri_hm_stats", "gci_rkpq_columns", "gci_dgemm_split",
+           "gci_dgemm", "gci_cholesky_inverse", "gci_trsm_rlt", "gci_autotune_eri",
            "gci_coulomb_grad", "gci_coulomb_grad_device", "gci_coulomb_grad_work", "gci_rkpq_batch")
 
 _pd = C.POINTER(C.c_double)
@@ -85,6 +86,9 @@ def lib():
         L.gci_rkpq_columns.argtypes = [C.c_void_p, _i64, _pl, _pd]
         L.gci_dgemm_split.argtypes = [_i64, _i64, _i64, C.c_double, C.c_void_p, _i64, C.c_void_p, _i64, C.c_double,
                                       C.c_void_p, _i64]
+        L.gci_dgemm.argtypes = L.gci_dgemm_split.argtypes
+        L.gci_cholesky_inverse.argtypes = [_i64, C.c_void_p, _i64, C.c_void_p]
+        L.gci_trsm_rlt.argtypes = [_i64, _i64, C.c_void_p, _i64, C.c_void_p, _i64]
         L.gci_autotune_eri.argtypes = [C.POINTER(gci_basis), C.c_int, _pd]
         L.gci_coulomb_grad.argtypes = [C.POINTER(gci_basis), C.c_double, _pd, _i64, _pd, _pd, _pd, _i64]
         L.gci_coulomb_grad_device.argtypes = [C.POINTER(gci_basis), C.c_double, C.c_void_p, _i64, _pd, _pd,

@@ -28,7 +28,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
 SOURCES = ["eri_kernels.cu", "eri_classes_a.cu", "eri_kf_a.cu", "eri_kf_b.cu", "eri_kf_c.cu", "eri_kf_d.cu",
            "grad_kernels.cu", "grad_pot_a.cu", "grad_pot_b.cu", "grad_pot_c.cu",
            "eri_hm_vectors.cu", "eri_hm_0.cu", "eri_hm_1.cu", "eri_hm_2.cu", "eri_hm_3.cu",
-           "eri_hm_4.cu", "eri_hm_5.cu", "eri_hm_6.cu", "chol_kernels.cu", "ozaki_gemm.cu", "gci_api.cu", "host_math.cpp"]
+           "eri_hm_4.cu", "eri_hm_5.cu", "eri_hm_6.cu", "chol_kernels.cu", "ozaki_gemm.cu", "dense_fp64.cu", "gci_api.cu", "host_math.cpp"]
 # ptxas at -O3 keeps the largest unrolled potential kernels (level sums >= 8)
 # entirely in local memory; -O1 allocates registers for them
 EXTRA = {"grad_pot_b.cu": ["-Xptxas", "-O1"], "grad_pot_c.cu": ["-Xptxas", "-O1"]}
@@ -86,15 +86,14 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         for f in [ex.submit(_compile, s, o, verbose) for s, o in todo]:
             f.result()
     if todo or not LIB.exists():
-        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcublas", "-lcusolver",
-               "-Xlinker", f"-rpath={CUDA_HOME / 'lib64'}"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-Xlinker", f"-rpath={CUDA_HOME / 'lib64'}"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     if todo or not ARCHIVE.exists():
         # the same objects as a static archive, for a Fortran build that links the
         # library into its own cholesky.a-based executable (the caller adds
-        # -lcudart -lcublas -lcusolver -lstdc++)
+        # -lcudart -lstdc++)
         if ARCHIVE.exists():
             ARCHIVE.unlink()
         r = subprocess.run(["ar", "rcs", str(ARCHIVE), *map(str, objs)], capture_output=True, text=True)

@@ -3,18 +3,20 @@
 //
 // Control flow follows the reference driver (TwoStepCholesky*.f90,
 // Cholesky_Gammcor.f90); the integral, pivot-search and contraction work
-// runs on the device (eri_kernels.cu, chol_kernels.cu, cuBLAS DGEMM for the
-// FP64 contractions, ozaki_gemm.cu for the split-precision int8 tensor-core GEMMs).
+// runs on the device (eri_kernels.cu and the Hermite-matrix kernels for the
+// integrals, chol_kernels.cu for the pivot search, dense_fp64.cu for the FP64
+// GEMMs, triangular solves and the V_JJ factorisation, ozaki_gemm.cu for the
+// split-precision int8 tensor-core GEMMs).  No vendor BLAS or solver library.
 #include "../../include/gci.h"
 #include "gci_common.h"
 #include "gci_runtime.h"
 #include "host_math.h"
-#include <cublas_v2.h>
-#include <cusolverDn.h>
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -35,16 +37,6 @@ struct Failure {
     do {                                                                                        \
         cudaError_t e_ = (x);                                                                   \
         if (e_ != cudaSuccess) fail(GCI_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-#define CB(x)                                                                                   \
-    do {                                                                                        \
-        cublasStatus_t s_ = (x);                                                                \
-        if (s_ != CUBLAS_STATUS_SUCCESS) fail(GCI_ERR_CUDA, std::string(#x) + " failed: " + std::to_string((int)s_)); \
-    } while (0)
-#define CS(x)                                                                                   \
-    do {                                                                                        \
-        cusolverStatus_t s_ = (x);                                                              \
-        if (s_ != CUSOLVER_STATUS_SUCCESS) fail(GCI_ERR_CUDA, std::string(#x) + " failed: " + std::to_string((int)s_)); \
     } while (0)
 
 template <class F>
@@ -145,14 +137,12 @@ struct Context {
     cudaStream_t aux[kAuxStreams] = {};
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_join[kAuxStreams] = {};
-    cublasHandle_t blas = nullptr;
-    cusolverDnHandle_t solver = nullptr;
     DVec<double> boys;
     DVec<int> err;
 };
 static Context g_ctx;
-// Worker contexts of gci_rkpq_batch (own stream, cuBLAS and cuSOLVER handles
-// and error word each; the Boys table is g_ctx's), kept for the process.
+// Worker contexts of gci_rkpq_batch (own stream and error word each; the Boys
+// table is g_ctx's), kept for the process.
 static std::vector<std::unique_ptr<Context>> g_pool;
 // Context of a batch worker thread; nullptr: the process-wide g_ctx.
 static thread_local Context* t_cur = nullptr;
@@ -161,11 +151,6 @@ static void context_streams(Context& c)
 {
     CU(cudaGetDevice(&c.device));
     CU(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-    CB(cublasCreate(&c.blas));
-    CB(cublasSetStream(c.blas, c.stream));
-    CB(cublasSetMathMode(c.blas, CUBLAS_DEFAULT_MATH));
-    CS(cusolverDnCreate(&c.solver));
-    CS(cusolverDnSetStream(c.solver, c.stream));
 }
 
 static Context& ctx()
@@ -859,11 +844,40 @@ static double accuracy_tau(int accuracy)
     }
 }
 
-static void gemm_nt(cublasHandle_t h, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,
-                    const double* B, int64_t ldb, double beta, double* Cm, int64_t ldc)
+// C = alpha A B^T + beta C, A (m x k), B (n x k), C (m x n) column-major, on the FP64
+// tensor-core GEMM (dense_fp64.cu); a_lower: A is lower triangular (Inv_L), its zero
+// upper part is skipped.
+static void gemm_nt(int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda, const double* B,
+                    int64_t ldb, double beta, double* Cm, int64_t ldc, bool a_lower = false)
 {
     if (m == 0 || n == 0) return;
-    CB(cublasDgemm_64(h, CUBLAS_OP_N, CUBLAS_OP_T, m, n, k, &alpha, A, lda, B, ldb, &beta, Cm, ldc));
+    DgemmArgs p{};
+    p.m = m; p.n = n; p.k = k; p.alpha = alpha; p.beta = beta;
+    p.a = A; p.sai = 1; p.sal = lda;
+    p.b = B; p.sbl = ldb; p.sbj = 1;
+    p.c = Cm; p.sci = 1; p.scj = ldc;
+    p.flags = a_lower ? kDgALower : 0;
+    CU(dgemm(p, 1, ctx().stream));
+}
+
+// C = alpha A B + beta C, all column-major (A m x k, B k x n), batched over `batch`
+// problems at element strides sab, sbb, scb.
+static void gemm_nn(int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda, int64_t sab,
+                    const double* B, int64_t ldb, int64_t sbb, double beta, double* Cm, int64_t ldc, int64_t scb,
+                    int64_t batch, bool a_lower = false)
+{
+    if (m == 0 || n == 0) return;
+    DgemmArgs p{};
+    p.m = m; p.n = n; p.k = k; p.alpha = alpha; p.beta = beta;
+    p.a = A; p.sai = 1; p.sal = lda; p.sab = sab;
+    p.b = B; p.sbl = 1; p.sbj = ldb; p.sbb = sbb;
+    p.c = Cm; p.sci = 1; p.scj = ldc; p.scb = scb;
+    p.flags = a_lower ? kDgALower : 0;
+    for (int64_t b0 = 0; b0 < batch; b0 += 65535) {
+        DgemmArgs q = p;
+        q.a += b0 * sab; q.b += b0 * sbb; q.c += b0 * scb;
+        CU(dgemm(q, std::min<int64_t>(65535, batch - b0), ctx().stream));
+    }
 }
 
 // Split-precision form of C = alpha A B^T + beta C on the int8 tensor cores
@@ -1045,14 +1059,18 @@ static void step1(Handle& H)
     DVec<double> dD, dD2;
     dD.upload(D, s);
     double dmax = *std::max_element(D.begin(), D.end());
-    // vector storage: Lst (ncand x cap), column-major, ld = ncand
-    int64_t cap = std::min<int64_t>(maxnchol, std::max<int64_t>(256, 4 * b.nao));
-    DVec<double> Lst, Lst2;
-    Lst.alloc((size_t)std::max<int64_t>(ncand, 1) * cap);
+    // vector storage over the candidates: blocks of kLBlk vectors, each ncand x kLBlk
+    // column-major (ld = ncand), allocated as the vectors arrive and re-gathered block by
+    // block when the candidates are compressed (the blocked V(b)%L of Step1.f90:1038-1041):
+    // the peak is the vectors themselves plus one block
+    constexpr int64_t kLBlk = 1024;
+    std::vector<DVec<double>> Lblk;
+    auto blk_cols = [&](size_t bi, int64_t nvec) { return std::min<int64_t>(kLBlk, nvec - (int64_t)bi * kLBlk); };
+    const bool trace = std::getenv("GCI_TRACE_STEP1") != nullptr;
     int64_t nchol = 0;
     bool converged = false, go = maxnchol > 0;
     int64_t nmacro = 0;
-    DVec<double> dM, dLB, dMbb, dDb, dLb, dpdmax, dLp, dsegmax, dscal;
+    DVec<double> dM, dLB, dMbb, dDb, dLb, dpdmax, dLp, dLnew, dsegmax, dscal;
     DVec<int> dpiv, dnpiv;
     DVec<int64_t> dgidx, dsegloc, dbrow;
     DVec<int> dsegdim;
@@ -1104,10 +1122,14 @@ static void step1(Handle& H)
             dD2.ensure(std::max<int64_t>(ncand_new, 1));
             CU(launch_gather_rows(dD.p, ncand, dgidx.p, ncand_new, 1, dD2.p, ncand_new, s));
             std::swap(dD, dD2);
-            if (nchol > 0 && ncand_new > 0) {
-                Lst2.ensure((size_t)ncand_new * cap);
-                CU(launch_gather_rows(Lst.p, ncand, dgidx.p, ncand_new, nchol, Lst2.p, ncand_new, s));
-                std::swap(Lst, Lst2);
+            if (ncand_new > 0) {
+                for (size_t bi = 0; bi < Lblk.size(); ++bi) {
+                    DVec<double> nb;
+                    nb.alloc((size_t)ncand_new * kLBlk);
+                    CU(launch_gather_rows(Lblk[bi].p, ncand, dgidx.p, ncand_new, blk_cols(bi, nchol), nb.p, ncand_new,
+                                          s));
+                    std::swap(Lblk[bi], nb);
+                }
             }
             for (size_t g = 0; g < ncand_list.size(); ++g) compr[ncand_list[g]] = newloc[g];
             cand = ncand_list;
@@ -1176,12 +1198,16 @@ static void step1(Handle& H)
             dbrow.upload(brow, s);
             T.start(kSubtractR);
             if (nchol > 0) {
-                dLB.ensure((size_t)nbatch * nchol);
-                CU(launch_gather_rows(Lst.p, ncand, dbrow.p, nbatch, nchol, dLB.p, nbatch, s));
-                if (H.flags & GCI_FLAG_MIXED_STEP1)
-                    gemm_nt_split(ncand, nbatch, nchol, -1.0, Lst.p, 1, ncand, dLB.p, 1, nbatch, 1.0, dM.p, ncand);
-                else
-                    gemm_nt(C.blas, ncand, nbatch, nchol, -1.0, Lst.p, ncand, dLB.p, nbatch, 1.0, dM.p, ncand);
+                dLB.ensure((size_t)nbatch * std::max<int64_t>(nchol, kLBlk));
+                for (size_t bi = 0; bi < Lblk.size(); ++bi) {
+                    const int64_t nc = blk_cols(bi, nchol);
+                    double* lb = dLB.p + (size_t)bi * kLBlk * nbatch;
+                    CU(launch_gather_rows(Lblk[bi].p, ncand, dbrow.p, nbatch, nc, lb, nbatch, s));
+                    if (H.flags & GCI_FLAG_MIXED_STEP1)
+                        gemm_nt_split(ncand, nbatch, nc, -1.0, Lblk[bi].p, 1, ncand, lb, 1, nbatch, 1.0, dM.p, ncand);
+                    else
+                        gemm_nt(ncand, nbatch, nc, -1.0, Lblk[bi].p, ncand, lb, nbatch, 1.0, dM.p, ncand);
+                }
                 H.gemm_flops[kGemmSubtractR] += 2.0 * ncand * nbatch * nchol;
             }
             T.stop();
@@ -1205,31 +1231,29 @@ static void step1(Handle& H)
                 CU(cudaMemcpyAsync(pdm.data(), dpdmax.p, sizeof(double) * npiv, cudaMemcpyDeviceToHost, s));
             }
             if (npiv > 0) {
-                if (nchol + npiv > cap) {
-                    int64_t ncap = std::min<int64_t>(maxnchol, std::max<int64_t>(2 * cap, nchol + npiv));
-                    DVec<double> nL;
-                    nL.alloc((size_t)std::max<int64_t>(ncand, 1) * ncap);
-                    if (nchol > 0)
-                        CU(cudaMemcpyAsync(nL.p, Lst.p, sizeof(double) * ncand * nchol, cudaMemcpyDeviceToDevice, s));
-                    std::swap(Lst, nL);
-                    Lst2.release();
-                    cap = ncap;
-                }
                 // vectors over all candidates: L_new Lp^T = M(:, piv), solved by forward
                 // substitution (the column-by-column recursion of chol2_Lj,
                 // Step1.f90:859-881, which stays backward stable when the batch
                 // holds nearly dependent pivots; an explicit inverse does not)
                 dLp.ensure((size_t)npiv * npiv);
                 CU(launch_gather_pivrows(dLb.p, (int)nbatch, dpiv.p, npiv, dLp.p, s));
-                double* Lnew = Lst.p + ncand * nchol;
-                CU(launch_gather_cols(dM.p, ncand, dpiv.p, ncand, npiv, Lnew, ncand, s));
-                {
-                    const double one = 1.0;
-                    CB(cublasDtrsm_64(C.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
-                                      CUBLAS_DIAG_NON_UNIT, ncand, npiv, &one, dLp.p, npiv, Lnew, ncand));
-                }
+                dLnew.ensure((size_t)ncand * npiv);
+                CU(launch_gather_cols(dM.p, ncand, dpiv.p, ncand, npiv, dLnew.p, ncand, s));
+                CU(trsm_rlt(ncand, npiv, dLnew.p, ncand, dLp.p, npiv, s));
                 H.gemm_flops[kGemmLnew] += (double)ncand * npiv * npiv;
-                CU(launch_downdate(dD.p, Lst.p + ncand * nchol, ncand, ncand, npiv, s));
+                CU(launch_downdate(dD.p, dLnew.p, ncand, ncand, npiv, s));
+                // append the new vectors to the blocks
+                for (int64_t j = 0; j < npiv;) {
+                    const int64_t col = nchol + j, bi = col / kLBlk, off = col % kLBlk;
+                    if (bi == (int64_t)Lblk.size()) {
+                        Lblk.emplace_back();
+                        Lblk.back().alloc((size_t)ncand * kLBlk);
+                    }
+                    const int64_t take = std::min<int64_t>(npiv - j, kLBlk - off);
+                    CU(cudaMemcpyAsync(Lblk[bi].p + off * ncand, dLnew.p + j * ncand, sizeof(double) * ncand * take,
+                                       cudaMemcpyDeviceToDevice, s));
+                    j += take;
+                }
             }
             T.stop();
             CU(cudaStreamSynchronize(s));
@@ -1246,6 +1270,13 @@ static void step1(Handle& H)
         CU(cudaStreamSynchronize(s));
         T.flush();
         if (ncand == 0) dmax = -1e300;
+        if (trace) {
+            size_t fr = 0, tot = 0;
+            cudaMemGetInfo(&fr, &tot);
+            std::fprintf(stderr, "step1 macro %lld: ncand %lld nbatch %lld nchol %lld dmax %.3e vectors %.2f GB free %.2f GB\n",
+                         (long long)nmacro, (long long)ncand, (long long)nbatch, (long long)nchol, dmax,
+                         8.0 * ncand * kLBlk * Lblk.size() / 1e9, fr / 1e9);
+        }
         if (dmax <= H.tau) { converged = true; go = false; }
         if (nchol == maxnchol || nbatch == 0) go = false;
     }
@@ -1328,29 +1359,19 @@ static void step2(Handle& H)
     T.stop();
     // real_Cholesky + real_LowerTriangularInverse (real_linalg.f90:39-72)
     T.start(kPotrf);
-    int lwork = 0;
-    CS(cusolverDnDpotrf_bufferSize(C.solver, CUBLAS_FILL_MODE_LOWER, (int)N, H.invl.p, (int)N, &lwork));
-    DVec<double> work;
-    work.alloc(std::max(lwork, 1));
-    DVec<int> info;
-    info.alloc(1);
-    CS(cusolverDnDpotrf(C.solver, CUBLAS_FILL_MODE_LOWER, (int)N, H.invl.p, (int)N, work.p, lwork, info.p));
-    int hinfo = 0;
-    CU(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
-    if (hinfo != 0) fail(GCI_ERR_NOT_SPD, "dpotrf failed: info=" + std::to_string(hinfo));
-    CU(launch_zero_upper(H.invl.p, N, s));
-    size_t wdev = 0, whost = 0;
-    CS(cusolverDnXtrtri_bufferSize(C.solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, N, CUDA_R_64F, H.invl.p, N,
-                                   &wdev, &whost));
-    DVec<char> wd;
-    wd.alloc(std::max<size_t>(wdev, 1));
-    std::vector<char> wh(std::max<size_t>(whost, 1));
-    CS(cusolverDnXtrtri(C.solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, N, CUDA_R_64F, H.invl.p, N, wd.p, wdev,
-                        wh.data(), whost, info.p));
-    CU(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
-    if (hinfo != 0) fail(GCI_ERR_NOT_SPD, "dtrtri failed: info=" + std::to_string(hinfo));
+    {
+        // L in place of V_JJ, Inv_L into a second buffer that becomes H.invl
+        DVec<double> X;
+        X.alloc((size_t)N * N);
+        DVec<int> info;
+        info.alloc(1);
+        CU(potrf_inverse(N, H.invl.p, X.p, N, info.p, s));
+        int hinfo = 0;
+        CU(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (hinfo != 0) fail(GCI_ERR_NOT_SPD, "Cholesky factorization of V_JJ failed: info=" + std::to_string(hinfo));
+        std::swap(H.invl, X);
+    }
     T.stop();
     H.gemm_flops[kGemmPotrf] += 2.0 * (double)N * N * N / 3.0;
     T.flush();
@@ -1394,7 +1415,7 @@ static void materialize_rkpq(Handle& H)
         H.timer.stop();
         // real_abT: Rkpq(:,:,X) = Inv_L W^T
         H.timer.start(kInvLGemm);
-        gemm_nt(C.blas, N, msd, N, 1.0, H.invl.p, N, W.p, msd, 0.0, H.rkpq.p + (size_t)N * msd * X, N);
+        gemm_nt(N, msd, N, 1.0, H.invl.p, N, W.p, msd, 0.0, H.rkpq.p + (size_t)N * msd * X, N, true);
         H.gemm_flops[kGemmInvL] += 2.0 * N * N * (double)msd;
         H.timer.stop();
     }
@@ -1408,15 +1429,11 @@ static void materialize_rkpq(Handle& H)
 static void mo_two_gemms(Handle& H, int precision, const double* U, int64_t kc, const double* CAd, int64_t NA,
                          const double* CBd, int64_t NB, double* W1, double* out, int64_t ldk)
 {
-    Context& C = ctx();
     const int64_t nao = H.hb.nao;
-    const double one = 1.0, zero = 0.0;
     H.gemm_flops[kGemmMo] += 2.0 * (double)nao * nao * kc * NA + 2.0 * (double)kc * NB * nao * NA;
     if (precision == GCI_PREC_FP64) {
-        CB(cublasDgemm_64(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, nao * kc, NA, nao, &one, U, nao * kc, CAd, nao, &zero, W1,
-                          nao * kc));
-        CB(cublasDgemmStridedBatched_64(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, kc, NB, nao, &one, W1, kc, nao * kc, CBd,
-                                        nao, 0, &zero, out, ldk * NA, ldk, NA));
+        gemm_nn(nao * kc, NA, nao, 1.0, U, nao * kc, 0, CAd, nao, 0, 0.0, W1, nao * kc, 0, 1);
+        gemm_nn(kc, NB, nao, 1.0, W1, kc, nao * kc, CBd, nao, 0, 0.0, out, ldk * NA, ldk, NA);
     } else {
         // W1 (nao kc x NA) = U (rows (q,k), K = p) C_A; then per a: out_a (kc x NB) = W1_a (kc x nao) C_B
         gemm_nt_split(nao * kc, NA, nao, 1.0, U, 1, nao * kc, CAd, nao, 1, 0.0, W1, nao * kc);
@@ -1491,9 +1508,25 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
             T.stop();
         }
     } else {
-        // direct: V(pq, J) chunks -> Vab(J, a, b) -> Rkab = Inv_L Vab
-        DVec<double> Vab;
-        Vab.alloc((size_t)N * NA * NB);
+        // direct: V(pq, J) chunks -> Vab(J, a, b) -> Rkab = Inv_L Vab.  The Vab rows of
+        // consecutive pivot chunks collect in Vc (vcap x NA NB, ld = vcap); a full Vc is
+        // multiplied into the output, Rkab(k, ab) += Inv_L(k, Jv0 + l) Vc(l, ab) for k >= Jv0
+        // (Inv_L is lower triangular), so no N x NA NB intermediate is held
+        const int64_t nab = NA * NB;
+        int64_t vcap = (int64_t)(4.0 * 1024.0 * 1024.0 * 1024.0 / (8.0 * (double)nab));
+        vcap = std::min<int64_t>(std::max<int64_t>(vcap, kc), N);
+        DVec<double> Vc;
+        Vc.alloc((size_t)vcap * nab);
+        int64_t Jv0 = 0, Jv1 = 0;   // pivot rows held in Vc
+        auto flush = [&]() {
+            if (Jv1 == Jv0) return;
+            T.start(kInvLGemm);
+            gemm_nn(N - Jv0, nab, Jv1 - Jv0, 1.0, H.invl.p + Jv0 + Jv0 * N, N, 0, Vc.p, vcap, 0, Jv0 == 0 ? 0.0 : 1.0,
+                    out_dev + Jv0, N, 0, 1, true);
+            H.gemm_flops[kGemmInvL] += 2.0 * (double)N * (double)(Jv1 - Jv0) * (double)nab;   // dense-GEMM count
+            T.stop();
+            Jv0 = Jv1;
+        };
         std::vector<int> baseids;
         for (int64_t s2 = 0; s2 < H.nsp; ++s2) baseids.push_back(H.bsp[s2]);
         int64_t k = 0;
@@ -1504,7 +1537,8 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
             if (k1 == k) ++k1;   // one pivot pair always fits (kc >= 1 pair of at most 49 columns)
             const int64_t J1 = H.psploc[k1 - 1] + H.pspdim[k1 - 1];
             const int64_t jc = J1 - J0;
-            if (jc > kc) fail(GCI_ERR_BUFFER, "Buffer size too small for Rpq->Rab");
+            if (jc > kc || jc > vcap) fail(GCI_ERR_BUFFER, "Buffer size too small for Rpq->Rab");
+            if (J1 - Jv0 > vcap) flush();
             PairMap cm;
             cm.reset(P.n);
             std::vector<int> kids;
@@ -1520,15 +1554,12 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
             run_eri(H, baseids, kids, kModeDense, nullptr, &cm, U.p, 0, jc);
             T.stop();
             T.start(kMoGemm);
-            mo_two_gemms(H, precision, U.p, jc, dCA.p, NA, dCB.p, NB, W1.p, Vab.p + J0, N);
+            mo_two_gemms(H, precision, U.p, jc, dCA.p, NA, dCB.p, NB, W1.p, Vc.p + (J0 - Jv0), vcap);
             T.stop();
+            Jv1 = J1;
             k = k1;
         }
-        T.start(kInvLGemm);
-        const double one = 1.0, zero = 0.0;
-        CB(cublasDgemm_64(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, N, NA * NB, N, &one, H.invl.p, N, Vab.p, N, &zero, out_dev, N));
-        H.gemm_flops[kGemmInvL] += 2.0 * (double)N * N * NA * NB;
-        T.stop();
+        flush();
     }
     if (precision == GCI_PREC_MIXED) check_device_error(C, "split-precision AO->MO");
     if (!device_io) CU(cudaMemcpyAsync(rkab, dOut.p, sizeof(double) * N * NA * NB, cudaMemcpyDeviceToHost, s));
@@ -1894,7 +1925,7 @@ int gci_rkpq_columns(gci_handle* h, int64_t n, const int64_t* pq, double* out)
         run_eri(H, ids, pivids, kModeProduct, &rows, &H.pivmap, W.p, n);
         // R(:, pq) = Inv_L W(pq, :)^T (TwoStepCholesky.f90:410-415 for these columns)
         R.alloc((size_t)N * n);
-        gemm_nt(C.blas, N, n, N, 1.0, H.invl.p, N, W.p, n, 0.0, R.p, N);
+        gemm_nt(N, n, N, 1.0, H.invl.p, N, W.p, n, 0.0, R.p, N, true);
         for (size_t d = 0; d < dup.size(); d += 2)
             CU(cudaMemcpyAsync(R.p + N * dup[d], R.p + N * dup[d + 1], sizeof(double) * N, cudaMemcpyDeviceToDevice,
                                s));
@@ -2115,6 +2146,53 @@ int gci_dgemm_split(int64_t m, int64_t n, int64_t k, double alpha, const double*
         gemm_nt_split(m, n, k, alpha, A, 1, lda, B, 1, ldb, beta, Cm, ldc);
         check_device_error(C, "gci_dgemm_split");
         pool_trim();
+    });
+}
+
+int gci_dgemm(int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda, const double* B,
+              int64_t ldb, double beta, double* Cm, int64_t ldc)
+{
+    if (m < 0 || n < 0 || k < 0 || lda < std::max<int64_t>(m, 1) || ldb < std::max<int64_t>(n, 1) ||
+        ldc < std::max<int64_t>(m, 1)) {
+        g_last_error = "invalid GEMM dimensions";
+        return GCI_ERR_ARG;
+    }
+    if ((m > 0 && n > 0) && (!Cm || (k > 0 && (!A || !B)))) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        Context& C = ctx();
+        gemm_nt(m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc);
+        CU(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int gci_cholesky_inverse(int64_t n, double* A, int64_t lda, double* X)
+{
+    if (n < 0 || lda < std::max<int64_t>(n, 1)) { g_last_error = "invalid dimensions"; return GCI_ERR_ARG; }
+    if (n > 0 && (!A || !X)) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        Context& C = ctx();
+        DVec<int> info;
+        info.alloc(1);
+        CU(potrf_inverse(n, A, X, lda, info.p, C.stream));
+        int hinfo = 0;
+        CU(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
+        CU(cudaStreamSynchronize(C.stream));
+        if (hinfo != 0) fail(GCI_ERR_NOT_SPD, "Cholesky factorization failed with exit code info=" + std::to_string(hinfo));
+        pool_trim();
+    });
+}
+
+int gci_trsm_rlt(int64_t rows, int64_t w, double* B, int64_t ldb, const double* L, int64_t ldl)
+{
+    if (rows < 0 || w < 0 || ldb < std::max<int64_t>(rows, 1) || ldl < std::max<int64_t>(w, 1)) {
+        g_last_error = "invalid dimensions";
+        return GCI_ERR_ARG;
+    }
+    if (rows > 0 && w > 0 && (!B || !L)) { g_last_error = "NULL argument"; return GCI_ERR_ARG; }
+    return guarded([&] {
+        Context& C = ctx();
+        CU(trsm_rlt(rows, w, B, ldb, L, ldl, C.stream));
+        CU(cudaStreamSynchronize(C.stream));
     });
 }
 

@@ -38,6 +38,32 @@ int64_t ozaki_max_k();
 cudaError_t ozaki_dgemm_nt(int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t ars, int64_t als,
                            const double* B, int64_t brs, int64_t bls, double beta, double* C, int64_t ldc,
                            void* work, int* err, cudaStream_t st);
+// FP64 dense kernels on the DMMA tensor path (dense_fp64.cu).
+// dgemm: C(i, j) = alpha sum_l A(i, l) B(l, j) + beta C(i, j) with A(i, l) = a[i sai + l sal],
+// B(l, j) = b[l sbl + j sbj], C(i, j) = c[i sci + j scj] (+ batch strides sab, sbb, scb per
+// batch index).  The flags declare structure whose zero part is skipped: kDgALower
+// (A(i, l) = 0 for l > i), kDgBLower (B(l, j) = 0 for l < j), kDgBUpper (B(l, j) = 0 for
+// l > j), kDgCLower (only C(i, j) with j <= i is written).  C must not overlap A or B.
+constexpr int kDgALower = 1, kDgBLower = 2, kDgBUpper = 4, kDgCLower = 8;
+struct DgemmArgs {
+    int64_t m, n, k;
+    double alpha, beta;
+    const double* a;
+    int64_t sai, sal, sab;
+    const double* b;
+    int64_t sbl, sbj, sbb;
+    double* c;
+    int64_t sci, scj, scb;
+    int flags;
+};
+cudaError_t dgemm(const DgemmArgs& p, int64_t batch, cudaStream_t st);
+// L (lower part of a, in place) and x = L^-1 (n x n, zeros above the diagonal) of the SPD
+// matrix a (lower part read), both column-major with leading dimension ld; *info = j + 1 for
+// the first non-positive pivot j found, else 0 (read it after the stream completes).  The
+// upper triangle of a is used as scratch.
+cudaError_t potrf_inverse(int64_t n, double* a, double* x, int64_t ld, int* info, cudaStream_t st);
+// b (rows x w, leading dimension ldb) <- b l^-T for the w x w lower-triangular l (ldl).
+cudaError_t trsm_rlt(int64_t rows, int64_t w, double* b, int64_t ldb, const double* l, int64_t ldl, cudaStream_t st);
 cudaError_t boys_eval_launch(int m, int64_t n, const double* x, const double* table, double* out, cudaStream_t st);
 
 cudaError_t launch_segmax(const double* D, const int64_t* loc, const int* dim, int64_t n, double* out, cudaStream_t s);

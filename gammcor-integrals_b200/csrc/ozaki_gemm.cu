@@ -17,10 +17,12 @@
 //  * k_oz_split: the seven slices of a block of rows, written in the tiled
 //    image the GEMM copies into shared memory unchanged (no swizzle, K-major
 //    canonical layout of 8-row x 16-byte core matrices);
-//  * k_oz_gemm: one 128 x 64 output tile per CTA; per 128-wide K block, one
-//    thread issues the 14 bulk copies (cp.async.bulk, mbarrier completion) of
-//    the A and B slice tiles and then 136 tcgen05.mma.kind::i8 (M=128, N=64,
-//    K=32) into the eight TMEM accumulators, committed to an mbarrier; the
+//  * k_oz_gemm: one 128 x 64 output tile per CTA, K in blocks of 64 through a
+//    two-stage shared-memory ring: one thread issues the 14 bulk copies
+//    (cp.async.bulk, mbarrier completion) of the next block's A and B slice
+//    tiles while the tensor core runs the 68 tcgen05.mma.kind::i8 (M=128,
+//    N=64, K=32) of the current block into the eight TMEM accumulators, each
+//    block's products committed to the mbarrier that frees its stage; the
 //    epilogue reads TMEM with tcgen05.ld and writes FP64.  Every wait is
 //    bounded: on expiry the CTA records GCI error 1, waits (bounded) for its
 //    own copies and products, frees its TMEM and returns.
@@ -31,11 +33,12 @@ namespace gci {
 
 constexpr int kOzSlices = 7;
 constexpr int kOzDMax = 9;                       // pairs with s + t <= 9
-constexpr int kOzAcc = kOzDMax - 1;              // accumulators d = 2..9
-constexpr int kOzBM = 128, kOzBN = 64, kOzBK = 128;
+constexpr int kOzBM = 128, kOzBN = 64, kOzBK = 64;
 constexpr int kOzTileA = kOzBM * kOzBK;          // bytes of one A slice tile
 constexpr int kOzTileB = kOzBN * kOzBK;
-constexpr int kOzSmem = kOzSlices * (kOzTileA + kOzTileB) + 64;
+constexpr int kOzStage = kOzSlices * (kOzTileA + kOzTileB);   // 84 KB: all slices of one K block
+constexpr int kOzStages = 2;
+constexpr int kOzSmem = kOzStages * kOzStage + 128;
 constexpr long long kOzSpin = 1LL << 28;         // bounded waits (~seconds)
 
 // ------------------------------------------------------------------ row exponents
@@ -53,7 +56,7 @@ __global__ void k_oz_rowexp(const double* __restrict__ X, int64_t rs, int64_t ls
 }
 
 // ------------------------------------------------------------------ slices
-// Tile (s, rb, kb) of R rows x 128 K bytes at ((s * nrb + rb) * nkb + kb) * R * 128;
+// Tile (s, rb, kb) of R rows x kOzBK (64) K bytes at ((s * nrb + rb) * nkb + kb) * R * 128;
 // inside a tile, byte (row, kk) at ((kk / 16) * (R / 8) + row / 8) * 128 + (row % 8) * 16 + kk % 16.
 template <int R>
 __global__ void k_oz_split(const double* __restrict__ X, int64_t rs, int64_t ls, int64_t rows, int64_t k,
@@ -163,7 +166,7 @@ struct OzArgs {
     const int8_t* b;       // B slice tiles (nrb_b row blocks of 64)
     const int* ea;         // row exponents of A (m) and B (n)
     const int* eb;
-    int64_t m, n, nkb;     // nkb: K blocks of 128
+    int64_t m, n, nkb;     // nkb: K blocks of kOzBK
     int64_t nrb_a, nrb_b;
     double alpha, beta;
     double* c;
@@ -174,17 +177,18 @@ struct OzArgs {
 __global__ void __launch_bounds__(128, 1) k_oz_gemm(const OzArgs p)
 {
     extern __shared__ __align__(1024) unsigned char oz_smem[];
-    int8_t* sa = reinterpret_cast<int8_t*>(oz_smem);
-    int8_t* sb = sa + kOzSlices * kOzTileA;
-    uint64_t* bar_load = reinterpret_cast<uint64_t*>(sb + kOzSlices * kOzTileB);
-    uint64_t* bar_mma = bar_load + 1;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_mma + 1);
+    uint64_t* bar_full = reinterpret_cast<uint64_t*>(oz_smem + kOzStages * kOzStage);   // per stage: copies landed
+    uint64_t* bar_empty = bar_full + kOzStages;                                         // per stage: products done
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_empty + kOzStages);
+    int* state = reinterpret_cast<int*>(tmem_slot + 1);   // ok, last committed block, last loaded block
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t cb = blockIdx.x, rb = blockIdx.y;
 
     if (threadIdx.x == 0) {
-        mbar_init(bar_load, 1);
-        mbar_init(bar_mma, 1);
+        for (int st = 0; st < kOzStages; ++st) {
+            mbar_init(bar_full + st, 1);
+            mbar_init(bar_empty + st, 1);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -199,19 +203,34 @@ __global__ void __launch_bounds__(128, 1) k_oz_gemm(const OzArgs p)
     const int64_t tsa = p.nrb_a * p.nkb * (int64_t)kOzTileA;   // stride between slices of A
     const int64_t tsb = p.nrb_b * p.nkb * (int64_t)kOzTileB;
     constexpr uint32_t idesc = umma_idesc_i8(kOzBM, kOzBN);
-    bool ok = true;
-    uint32_t phase = 0;
-    for (int64_t kb = 0; kb < p.nkb && ok; ++kb) {
-        if (threadIdx.x == 0) {
-            mbar_expect_tx(bar_load, kOzSlices * (kOzTileA + kOzTileB));
+    if (threadIdx.x == 0) {
+        // block kb lives in stage kb % 2; its copies complete phase (kb / 2) % 2 of
+        // bar_full[stage], its products phase (kb / 2) % 2 of bar_empty[stage]
+        auto load = [&](int64_t kb) {
+            const int st = (int)(kb & 1);
+            int8_t* sa = reinterpret_cast<int8_t*>(oz_smem + st * kOzStage);
+            int8_t* sb = sa + kOzSlices * kOzTileA;
+            mbar_expect_tx(bar_full + st, kOzStage);
             for (int s = 0; s < kOzSlices; ++s) {
-                bulk_copy(sa + s * kOzTileA, p.a + s * tsa + (rb * p.nkb + kb) * kOzTileA, kOzTileA, bar_load);
-                bulk_copy(sb + s * kOzTileB, p.b + s * tsb + (cb * p.nkb + kb) * kOzTileB, kOzTileB, bar_load);
+                bulk_copy(sa + s * kOzTileA, p.a + s * tsa + (rb * p.nkb + kb) * kOzTileA, kOzTileA, bar_full + st);
+                bulk_copy(sb + s * kOzTileB, p.b + s * tsb + (cb * p.nkb + kb) * kOzTileB, kOzTileB, bar_full + st);
             }
-        }
-        ok = mbar_wait(bar_load, phase);
-        if (threadIdx.x == 0 && ok) {
+        };
+        bool ok = true;
+        int64_t last_commit = -1, last_load = 0;
+        load(0);
+        for (int64_t kb = 0; kb < p.nkb; ++kb) {
+            const int st = (int)(kb & 1);
+            if (kb + 1 < p.nkb) {
+                // the other stage is free once the products of block kb - 1 are done
+                if (kb >= 1 && !(ok = mbar_wait(bar_empty + (st ^ 1), (uint32_t)(((kb - 1) >> 1) & 1)))) break;
+                load(kb + 1);
+                last_load = kb + 1;
+            }
+            if (!(ok = mbar_wait(bar_full + st, (uint32_t)((kb >> 1) & 1)))) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int8_t* sa = reinterpret_cast<const int8_t*>(oz_smem + st * kOzStage);
+            const int8_t* sb = sa + kOzSlices * kOzTileA;
             for (int d = 2; d <= kOzDMax; ++d) {
                 const uint32_t td = tmem + (uint32_t)((d - 2) * kOzBN);
                 bool first = kb == 0;
@@ -229,17 +248,27 @@ __global__ void __launch_bounds__(128, 1) k_oz_gemm(const OzArgs p)
                     }
                 }
             }
-            umma_commit(bar_mma);
+            umma_commit(bar_empty + st);
+            last_commit = kb;
         }
-        if (ok) ok = mbar_wait(bar_mma, phase);
-        phase ^= 1;
-        ok = __syncthreads_and(ok);
+        state[0] = ok ? 1 : 0;
+        state[1] = (int)last_commit;
+        state[2] = (int)last_load;
     }
+    __syncthreads();
+    bool ok = state[0] != 0;
+    const int64_t last_commit = state[1], last_load = state[2];
+    if (ok) ok = mbar_wait(bar_empty + (last_commit & 1), (uint32_t)((last_commit >> 1) & 1));
+    ok = __syncthreads_and(ok);
     if (!ok) {
-        if (threadIdx.x == 0) atomicCAS(p.err, 0, 1);
-        // let copies and products already issued finish (bounded) before the TMEM goes
-        mbar_wait(bar_load, phase ^ 1);
-        mbar_wait(bar_mma, phase ^ 1);
+        if (threadIdx.x == 0) {
+            atomicCAS(p.err, 0, 1);
+            // let copies and products already issued finish (bounded) before the TMEM goes
+            // (both stages: a block whose copies already landed passes at once)
+            for (int64_t kb = last_load - 1; kb <= last_load; ++kb)
+                if (kb >= 0) mbar_wait(bar_full + (kb & 1), (uint32_t)((kb >> 1) & 1));
+            if (last_commit >= 0) mbar_wait(bar_empty + (last_commit & 1), (uint32_t)((last_commit >> 1) & 1));
+        }
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         // epilogue: thread (warp w, lane l) owns row 32 w + l of the tile

@@ -5,7 +5,7 @@
 ! the C ABI of include/gci.h.
 !
 ! Build: compile this file in place of Cholesky_Gammcor.f90 into the
-! cholesky.a archive, and link libgci.so (with -lcublas -lcusolver -lcudart).
+! cholesky.a archive, and link libgci.so (with -lcudart).
 ! The modules it uses (arithmetic, display, TwoStepCholesky_definitions,
 ! basis_definitions, Auto2eInterface) are the reference's own.
 !

@@ -25,7 +25,7 @@ extern "C" {
 /* status codes */
 #define GCI_OK                 0
 #define GCI_ERR_ARG           -1   /* invalid argument / dimension       */
-#define GCI_ERR_CUDA          -2   /* CUDA, cuBLAS or cuSOLVER failure    */
+#define GCI_ERR_CUDA          -2   /* CUDA runtime or kernel launch failure */
 #define GCI_ERR_UNSUPPORTED   -3   /* angular momentum beyond the kernels, or a mode not built */
 #define GCI_ERR_NOT_CONVERGED -4   /* MaxNCholesky reached unconverged    */
 #define GCI_ERR_NOT_SPD       -5   /* pivot block V_JJ not positive definite */
@@ -46,7 +46,7 @@ extern "C" {
 #define GCI_FLAG_MIXED_STEP1        4  /* M - L L^T of the pivot search (chol2_SubtractR) as a split-precision
                                           GEMM on the int8 tensor cores (gci_dgemm_split) */
 
-/* Precision of the AO->MO GEMMs: FP64 (cuBLAS DGEMM) or split precision on the int8
+/* Precision of the AO->MO GEMMs: FP64 (DMMA tensor-core GEMM) or split precision on the int8
  * tensor cores (gci_dgemm_split) */
 #define GCI_PREC_FP64   0
 #define GCI_PREC_MIXED  1
@@ -89,7 +89,7 @@ int gci_rkpq(const gci_basis *basis, int accuracy, double omega, int flags, gci_
 /* gci_rkpq for many independent molecules at once (the reference decomposes one molecule per
  * chol_gammcor_Rkpq call, Cholesky_Gammcor.f90:335-377).  The molecules are taken largest
  * first from one queue by nstreams host workers (<= 0: 16; at most 64), each with its own
- * CUDA stream and cuBLAS/cuSOLVER handles, so that the kernels of different molecules run
+ * CUDA stream, so that the kernels of different molecules run
  * concurrently on the GPU.  out[i] receives the handle of bases[i] (same results as gci_rkpq
  * on that basis).  On an error no handle is returned (all out[i] = NULL) and
  * gci_last_error() names the lowest-index molecule that failed.  Batch calls from
@@ -146,7 +146,7 @@ int gci_rkab_device(gci_handle *h, const double *CA, int64_t ldca, int64_t a0, i
  * Pair type of (l_hi, l_lo) = l_hi(l_hi+1)/2 + l_lo. */
 int gci_stats(const gci_handle *h, double *out, int n);
 
-/* Kernels of this library launched so far in the process (cuBLAS/cuSOLVER calls excluded). */
+/* Kernels of this library launched so far in the process. */
 int gci_kernel_launches(int64_t *n);
 
 /* The CUDA stream (cudaStream_t) every call of the library runs on. */
@@ -201,6 +201,29 @@ int gci_eri_variant(int tb, int tk, int variant);
 int gci_dgemm_split(int64_t m, int64_t n, int64_t k, double alpha, const double *A, int64_t lda,
                     const double *B, int64_t ldb, double beta, double *C, int64_t ldc);
 
+/* ---- FP64 dense kernels of the decomposition (DMMA tensor cores, mma.sync m8n8k4 f64) ----
+ * Like gci_dgemm_split these run on the library's stream (gci_get_stream), which does not wait
+ * for the caller's streams: the inputs must be complete before the call.  They return after
+ * the results are complete. */
+
+/* C = alpha A B^T + beta C in FP64, same argument convention as gci_dgemm_split (the
+ * dgemm("N", "T", ...) calls of real_linalg.f90:1331-1361, e.g. chol2_SubtractR,
+ * TwoStepCholesky_Step1.f90:628-691).  DEVICE pointers, library stream. */
+int gci_dgemm(int64_t m, int64_t n, int64_t k, double alpha, const double *A, int64_t lda, const double *B,
+              int64_t ldb, double beta, double *C, int64_t ldc);
+
+/* real_Cholesky + real_LowerTriangularInverse (real_linalg.f90:39-72, dpotrf("L") then
+ * dtrtri("L", "N")): A (n x n, lda, lower triangle read) is overwritten by L in its lower
+ * triangle (its upper triangle is used as scratch); X (n x n, ldx = lda) receives L^-1 with
+ * zeros above the diagonal.  DEVICE pointers.  GCI_ERR_NOT_SPD when a pivot is not
+ * positive (the reference stops with "Cholesky factorization failed"). */
+int gci_cholesky_inverse(int64_t n, double *A, int64_t lda, double *X);
+
+/* B (rows x w, ldb) <- B L^-T for the w x w lower-triangular L (ldl): dtrsm("R", "L", "T",
+ * "N") as used for the vectors of a pivot batch (chol2_Lj, TwoStepCholesky_Step1.f90:859-881).
+ * DEVICE pointers. */
+int gci_trsm_rlt(int64_t rows, int64_t w, double *B, int64_t ldb, const double *L, int64_t ldl);
+
 /* Hermite-matrix ERI kernels (default on).  For spherical bases the
  * product-mode stages (step-1 pivot columns, the pivot block, the
  * full-dimension stage, gci_eri_pairs) contract each pair's primitive
@@ -215,7 +238,7 @@ int gci_eri_hm(int enable);
 
 /* Work of the Hermite-matrix kernels of a decomposition (and its gci_rkab
  * calls): for every row level L1 (0..6), column level L2 (0..6) and column
- * tile count (1..7, at most 7 for L1 <= 3, 4 for L1 = 4, 3 above), in that
+ * tile count (1..7, at most 7 for L1 <= 3, 5 for L1 = 4, 4 for L1 = 5, 3 for L1 = 6), in that
  * order: launches, device seconds (measured only with gci_eri_hm(2)) and
  * tensor-core flops issued (padding included); 7 x 7 x 7 x 3 values. */
 int gci_eri_hm_stats(const gci_handle *h, double *out, int n);
