@@ -1466,7 +1466,15 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
     CU(cudaMemcpy2DAsync(dCB.p, sizeof(double) * nao, CB_ + ldcb * (b0 - 1), sizeof(double) * ldcb,
                          sizeof(double) * nao, NB, kind, s));
     double* out_dev = rkab;
-    if (!device_io) {
+    // host output too large for the device next to Inv_L and the integral buffers: the
+    // direct path stages Vab in the caller's host array and applies Inv_L column block by
+    // column block from there (out of core)
+    size_t free_b = 0, total_b = 0;
+    CU(cudaMemGetInfo(&free_b, &total_b));
+    // (GCI_RKAB_OUT_OF_CORE in the environment forces it, for tests)
+    const bool ooc = !device_io && !H.have_rkpq &&
+                     (8.0 * (double)N * NA * NB > 0.5 * (double)free_b || std::getenv("GCI_RKAB_OUT_OF_CORE"));
+    if (!device_io && !ooc) {
         dOut.alloc((size_t)N * NA * NB);
         out_dev = dOut.p;
     }
@@ -1520,6 +1528,13 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
         int64_t Jv0 = 0, Jv1 = 0;   // pivot rows held in Vc
         auto flush = [&]() {
             if (Jv1 == Jv0) return;
+            if (ooc) {
+                // rows Jv0..Jv1 of Vab into the host array (final layout, ld = N)
+                CU(cudaMemcpy2DAsync(rkab + Jv0, sizeof(double) * N, Vc.p, sizeof(double) * vcap,
+                                     sizeof(double) * (Jv1 - Jv0), nab, cudaMemcpyDeviceToHost, s));
+                Jv0 = Jv1;
+                return;
+            }
             T.start(kInvLGemm);
             gemm_nn(N - Jv0, nab, Jv1 - Jv0, 1.0, H.invl.p + Jv0 + Jv0 * N, N, 0, Vc.p, vcap, 0, Jv0 == 0 ? 0.0 : 1.0,
                     out_dev + Jv0, N, 0, 1, true);
@@ -1560,9 +1575,30 @@ static void rkab_impl(Handle& H, const double* CA, int64_t ldca, int64_t a0, int
             k = k1;
         }
         flush();
+        if (ooc) {
+            // Rkab(:, c) = Inv_L Vab(:, c) for blocks of columns c, in place in the host array
+            Vc.release();
+            U.release();
+            W1.release();
+            CU(cudaMemGetInfo(&free_b, &total_b));
+            int64_t w = (int64_t)std::min(0.4 * (double)free_b, 16.0 * 1024 * 1024 * 1024) / (16 * N);
+            w = std::max<int64_t>(1, std::min(w, nab));
+            DVec<double> Vin, Vout;
+            Vin.alloc((size_t)N * w);
+            Vout.alloc((size_t)N * w);
+            T.start(kInvLGemm);
+            for (int64_t c0 = 0; c0 < nab; c0 += w) {
+                const int64_t cw = std::min(w, nab - c0);
+                CU(cudaMemcpyAsync(Vin.p, rkab + c0 * N, sizeof(double) * N * cw, cudaMemcpyHostToDevice, s));
+                gemm_nn(N, cw, N, 1.0, H.invl.p, N, 0, Vin.p, N, 0, 0.0, Vout.p, N, 0, 1, true);
+                CU(cudaMemcpyAsync(rkab + c0 * N, Vout.p, sizeof(double) * N * cw, cudaMemcpyDeviceToHost, s));
+            }
+            H.gemm_flops[kGemmInvL] += 2.0 * (double)N * (double)N * (double)nab;
+            T.stop();
+        }
     }
     if (precision == GCI_PREC_MIXED) check_device_error(C, "split-precision AO->MO");
-    if (!device_io) CU(cudaMemcpyAsync(rkab, dOut.p, sizeof(double) * N * NA * NB, cudaMemcpyDeviceToHost, s));
+    if (!device_io && !ooc) CU(cudaMemcpyAsync(rkab, dOut.p, sizeof(double) * N * NA * NB, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     T.flush();
 }

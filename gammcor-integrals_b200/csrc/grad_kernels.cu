@@ -4,6 +4,7 @@
 // instantiated in grad_pot_*.cu).
 #include "grad_engine.cuh"
 #include "gci_runtime.h"
+#include <mutex>
 
 namespace gci {
 
@@ -230,12 +231,13 @@ static GradLaunchFn g_grad_launch[kGradMaxL + 1][kGradMaxL + 1];
 
 cudaError_t grad_module_init()
 {
-    static bool done = false;
-    if (done) return cudaSuccess;
-    register_grad_pot_a(g_grad_launch);
-    register_grad_pot_b(g_grad_launch);
-    register_grad_pot_c(g_grad_launch);
-    done = true;
+    // the table is filled once; concurrent first calls wait for it
+    static std::once_flag once;
+    std::call_once(once, [] {
+        register_grad_pot_a(g_grad_launch);
+        register_grad_pot_b(g_grad_launch);
+        register_grad_pot_c(g_grad_launch);
+    });
     return cudaSuccess;
 }
 

@@ -249,3 +249,19 @@ def test_c1_job_parity(gpu_lib):
     assert np.max(np.abs(got2 - ref)) < 1e-8
     O.free(ch)
     O.free(ch2)
+
+
+def test_rkab_out_of_core_matches(gpu_lib, monkeypatch):
+    """The direct AO->MO path with Vab staged in the caller's host array and Inv_L applied
+    block by block from there (used when the host output does not fit on the device;
+    forced here by GCI_RKAB_OUT_OF_CORE) gives the in-core result; an 8 MB buffer splits
+    the full-dimension integrals into several pivot chunks."""
+    mol = molecules.config("c1")
+    tb, _ = both(mol)
+    res = cg.chol_gammcor_Rkpq(tb, cg.CHOL_ACCURACY_TIGHT, materialize=False)
+    nocc, nvirt, seed = molecules.MO_SPLIT["c1"]
+    Cm = molecules.mo_coefficients(tb.NAO, seed)
+    ref = cg.chol_gammcor_Rkab(Cm, 1, nocc, Cm, nocc + 1, nocc + nvirt, 1024, res, tb)
+    monkeypatch.setenv("GCI_RKAB_OUT_OF_CORE", "1")
+    got = cg.chol_gammcor_Rkab(Cm, 1, nocc, Cm, nocc + 1, nocc + nvirt, 8, res, tb)
+    assert np.max(np.abs(got - ref)) < 1e-11
