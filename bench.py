@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--hm-profile", action="store_true",
                     help="diagnostic: time every Hermite-matrix class launch (serialised) and print the table")
     ap.add_argument("--streams", type=int, default=32, help="c3: workers (CUDA streams) of gci_rkpq_batch")
+    ap.add_argument("--dense", action="store_true",
+                    help="time the library's FP64 dense kernels (gci_dgemm, gci_cholesky_inverse, gci_trsm_rlt) "
+                         "and the split-precision GEMM against torch/cuBLAS/cuSOLVER at fixed shapes")
     ap.add_argument("--decode-storage", action="store_true",
                     help="decode diagonal-shell-pair pivots in storage order (GCI_FLAG_PIVOT_DECODE_STORAGE)")
     return ap.parse_args()
@@ -512,6 +515,87 @@ def run_batch(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_dense(args):
+    """The dense kernels of the decomposition alone, on one GPU: each shape timed with CUDA
+    events (best of 3 after one warm-up) next to the vendor library doing the same job
+    (torch.matmul = cuBLAS DGEMM; torch.linalg.cholesky + solve_triangular = cuSOLVER), and
+    the largest difference of the results."""
+    import ctypes as C
+    import torch
+    import gammcor_pkg
+    gammcor_pkg.load()
+    from gammcor_integrals_b200 import _capi
+    L = _capi.lib()
+    _capi.check(L.gci_init())
+    vp = lambda t: C.c_void_p(t.data_ptr())
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(3):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            best = min(best, time.perf_counter() - t0)
+        return best
+
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(11)
+    for m, n, k in ((8192, 8192, 8192), (200000, 1000, 1024), (16285, 2000, 16285)):
+        At = torch.randn(k, m, dtype=torch.float64, device="cuda", generator=g)
+        Bt = torch.randn(k, n, dtype=torch.float64, device="cuda", generator=g)
+        Ct = torch.empty(n, m, dtype=torch.float64, device="cuda")
+        t_ours = timed(lambda: _capi.check(L.gci_dgemm(m, n, k, 1.0, vp(At), m, vp(Bt), n, 0.0, vp(Ct), m)))
+        t_lib = timed(lambda: torch.matmul(At.T, Bt))
+        err = float((Ct.T - At.T @ Bt).abs().max())
+        t_split = timed(lambda: _capi.check(L.gci_dgemm_split(m, n, k, 1.0, vp(At), m, vp(Bt), n, 0.0, vp(Ct),
+                                                              m)))
+        err_split = float((Ct.T - At.T @ Bt).abs().max())
+        f = 2.0 * m * n * k / 1e12
+        out[f"gemm_nt {m}x{n}x{k}"] = {"k_dgemm_tflops": f / t_ours, "cublas_dgemm_tflops": f / t_lib,
+                                       "k_dgemm_max_abs_diff": err, "split_int8_tflops_fp64_equivalent": f / t_split,
+                                       "split_max_abs_diff": err_split}
+        del At, Bt, Ct
+        torch.cuda.empty_cache()
+    for nn in (4096, 16285):
+        X0 = torch.randn(nn, nn, dtype=torch.float64, device="cuda", generator=g)
+        S = X0 @ X0.T / nn + torch.eye(nn, dtype=torch.float64, device="cuda")
+        del X0
+        A, X = torch.empty_like(S), torch.empty_like(S)
+        eye = torch.eye(nn, dtype=torch.float64, device="cuda")
+
+        def ours():
+            A.copy_(S)
+            torch.cuda.synchronize()
+            _capi.check(L.gci_cholesky_inverse(nn, vp(A), nn, vp(X)))
+
+        t_ours = timed(ours) - timed(lambda: A.copy_(S))
+        t_lib = timed(lambda: torch.linalg.solve_triangular(torch.linalg.cholesky(S), eye, upper=False))
+        Xr = torch.linalg.solve_triangular(torch.linalg.cholesky(S), eye, upper=False)
+        out[f"cholesky_inverse {nn}"] = {"ours_s": t_ours, "cusolver_potrf_plus_trsm_s": t_lib,
+                                         "max_rel_diff": float((X.T - Xr).abs().max() / Xr.abs().max())}
+        del S, A, X, eye, Xr
+        torch.cuda.empty_cache()
+    rows, w = 600000, 400
+    Z = torch.randn(w, w, dtype=torch.float64, device="cuda", generator=g)
+    Lp = torch.linalg.cholesky(Z @ Z.T / w + torch.eye(w, dtype=torch.float64, device="cuda"))
+    B0 = torch.randn(w, rows, dtype=torch.float64, device="cuda", generator=g)
+    B, Lt = B0.clone(), Lp.T.contiguous()
+
+    def ours_trsm():
+        B.copy_(B0)
+        torch.cuda.synchronize()
+        _capi.check(L.gci_trsm_rlt(rows, w, vp(B), rows, vp(Lt), w))
+
+    t_ours = timed(ours_trsm) - timed(lambda: B.copy_(B0))
+    t_lib = timed(lambda: torch.linalg.solve_triangular(Lp, B0, upper=False))
+    ref = torch.linalg.solve_triangular(Lp, B0, upper=False)
+    out[f"trsm_rlt {rows}x{w}"] = {"ours_s": t_ours, "cublas_trsm_s": t_lib, "max_abs_diff": float((B - ref).abs().max())}
+    print(json.dumps({"dense_kernels": out, "note": "wall time around each call with a device synchronisation; "
+                      "the library calls include their argument checks and stream synchronisation"}), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -519,6 +603,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.dense:
+        if rank == 0:
+            run_dense(args)
         return
     if args.config == "c3":
         if rank == 0:
@@ -564,7 +652,7 @@ def main():
     _capi.check(L.gci_get_stream(C.byref(sptr)))
     lib_stream = torch.cuda.ExternalStream(sptr.value)
     bstruct = tb.c_struct()
-    state = {"rkab": None, "nvecs": None}
+    state = {"rkab": None, "nvecs": None, "parts": None}
     # per-class kernel choice (team vs ket-first) by the library's autotuner, untimed set-up
     tune = np.zeros(400)
     t_tune = time.perf_counter()
@@ -582,10 +670,22 @@ def main():
         nv = C.c_int64()
         _capi.check(L.gci_query(h, C.byref(nv), None, None, None, None, None))
         if state["rkab"] is None or state["nvecs"] != nv.value:
-            state["rkab"] = torch.empty(nv.value * NA * NB, dtype=torch.float64, device="cuda")
+            state["rkab"] = None
+            # Rkab on the device, in one piece when it fits beside the library's own buffers
+            # (Inv_L, the integral chunks); otherwise in ranges of virtual orbitals, one
+            # gci_rkab_device call each into the same buffer (c5: 48k vectors x 150 x 2700 =
+            # 156 GB, more than the HBM and than 80% of the host memory of the box)
+            free = torch.cuda.mem_get_info()[0]
+            nparts = 1
+            while 8.0 * nv.value * NA * -(-NB // nparts) > 0.55 * free:
+                nparts += 1
+            nbp = -(-NB // nparts)
+            state["parts"] = [(b0 + q * nbp, min(b1, b0 + (q + 1) * nbp - 1)) for q in range(nparts)]
+            state["rkab"] = torch.empty(nv.value * NA * nbp, dtype=torch.float64, device="cuda")
             state["nvecs"] = nv.value
-        _capi.check(L.gci_rkab_device(h, C.c_void_p(c_dev.data_ptr()), nao, a0, a1, C.c_void_p(c_dev.data_ptr()),
-                                      nao, b0, b1, args.buffer_mb, prec, C.c_void_p(state["rkab"].data_ptr())))
+        for pb0, pb1 in state["parts"]:
+            _capi.check(L.gci_rkab_device(h, C.c_void_p(c_dev.data_ptr()), nao, a0, a1, C.c_void_p(c_dev.data_ptr()),
+                                          nao, pb0, pb1, args.buffer_mb, prec, C.c_void_p(state["rkab"].data_ptr())))
         st = np.zeros(8 + 600 + 1)
         _capi.check(L.gci_stats(h, _capi.ptr(st), st.size))
         tm = np.zeros(13)
@@ -647,12 +747,14 @@ def main():
     # parity tests (tests/test_gpu_parity.py); a split-precision run is compared here
     # with the FP64 path on the same molecule
     err = {"fp64_path": "parity with the FP64 oracle: tests/test_gpu_parity.py"}
-    if args.precision != "fp64":
+    if args.precision != "fp64" and len(state["parts"]) > 1:
+        err["mixed_vs_fp64"] = "not measured: the two outputs do not fit on the device together"
+    elif args.precision != "fp64":
         err.update(mixed_vs_fp64(L, bstruct, c_dev, nao, a0, a1, b0, b1, args.buffer_mb, state, torch))
 
     # ---- end to end through the public host API (pinned host buffers)
     e2e = None
-    if args.e2e_steps > 0:
+    if args.e2e_steps > 0 and len(state["parts"]) == 1:   # host output of the whole Rkab
         nv = state["nvecs"]
         pin_c = torch.from_numpy(np.ascontiguousarray(Cm.T)).pin_memory()
         pin_out = torch.empty(nv * NA * NB, dtype=torch.float64).pin_memory()
@@ -704,6 +806,9 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload_name(args.config), "precision": args.precision,
                        "nvecs": state["nvecs"], "parallelism": f"replicas x{world}",
+                       "rkab_output": ("device (gci_rkab_device)" if len(state["parts"]) == 1 else
+                                       f"device, in {len(state['parts'])} ranges of virtual orbitals (one "
+                                       f"gci_rkab_device call each; the whole Rkab exceeds the HBM)"),
                        "l2": "flushed before every timed step (512 MB write outside the timed events)"},
             "value_definition": "device seconds of one complete job (decomposition + AO->MO) on each GPU, "
                                 "CUDA events on the library stream, max over ranks",

@@ -1,11 +1,14 @@
-"""GPU parity at the c2 configuration (40 atoms, NAO = 1200, tau = 1e-6) on a
-seeded sample: the Cholesky vectors of the orbital pairs of a few BASE shell
-pairs of every pair type (gci_rkpq_columns, no materialised Rkpq) reconstruct
-the exact integrals (pq|rs) of the oracle within the decomposition's own
-bound tau (|V - L L^T| <= sqrt(D_pq D_rs) <= tau at convergence,
-TwoStepCholesky_Step1.f90:884-1103).  This checks the pivot search, the pivot
-block, Inv_L and the full-dimension integrals of the real configuration,
-which the oracle cannot decompose in test time."""
+"""GPU parity at the c2 configuration (40 atoms, NAO = 1200, tau = 1e-6) and,
+when GCI_TEST_C5 is set in the environment (a four-minute decomposition), at
+c5 (120 atoms, NAO = 3600), on a seeded sample: the Cholesky vectors of the
+orbital pairs of a few BASE shell pairs of every pair type (gci_rkpq_columns,
+no materialised Rkpq) reconstruct the exact integrals (pq|rs) of the oracle
+within the decomposition's own bound tau (|V - L L^T| <= sqrt(D_pq D_rs) <=
+tau at convergence, TwoStepCholesky_Step1.f90:884-1103).  This checks the
+pivot search, the pivot block, Inv_L and the full-dimension integrals of the
+real configuration, which the oracle cannot decompose in test time."""
+import os
+
 import numpy as np
 import pytest
 
@@ -23,8 +26,11 @@ def _stored_functions(same: bool, na: int, nb: int):
     return [(a, b) for b in range(nb) for a in range(b if same else 0, na)]
 
 
-def test_c2_sampled_reconstruction(gpu_lib):
-    mol = molecules.config("c2")
+@pytest.mark.parametrize("config", ["c2", "c5"])
+def test_sampled_reconstruction(gpu_lib, config):
+    if config == "c5" and not os.environ.get("GCI_TEST_C5"):
+        pytest.skip("c5 runs only with GCI_TEST_C5 set")
+    mol = molecules.config(config)
     tb, ob = both(mol)
     res = cg.chol_gammcor_Rkpq(tb, cg.CHOL_ACCURACY_TIGHT, materialize=False)
     d = res.Chol2Data
