@@ -51,8 +51,9 @@ def parse():
     ap.add_argument("--tune-pairs", type=int, default=40, help="shell pairs per class sampled by the ERI autotuner")
     ap.add_argument("--eri-kernels", default="hermite", choices=["hermite", "class"],
                     help="product stages on the Hermite-matrix tensor-core kernels or the per-class kernels")
-    ap.add_argument("--dump-work", action="store_true",
-                    help="record the job's per-class work counts in oracle/job_work.json (reference-arm input)")
+    ap.add_argument("--dump-work", nargs="?", const=str(ROOT / "oracle" / "job_work.json"), default=None,
+                    metavar="PATH", help="record the job's per-class work counts (reference-arm input) in PATH, "
+                                         "by default oracle/job_work.json")
     ap.add_argument("--hm-profile", action="store_true",
                     help="diagnostic: time every Hermite-matrix class launch (serialised) and print the table")
     ap.add_argument("--streams", type=int, default=32, help="c3: workers (CUDA streams) of gci_rkpq_batch")
@@ -461,7 +462,11 @@ def run_batch(args, local):
         _capi.check(L.gci_rkpq_batch(64, arr, _capi.GCI_ACCURACY_DEFAULT, 0.0, 0, nstreams, hs))
         return hs
 
-    def stats_of(hs):
+    phase_names = ("vdiag", "step1_eri", "subtract_r", "pivots", "compress", "vjj_eri", "potrf_trtri")
+    phase_sum = dict.fromkeys(phase_names, 0.0)
+    extra = {"rkpq_host_s": 0.0, "macro_iterations": 0.0}
+
+    def stats_of(hs, record=False):
         tot = 0.0
         nv = []
         for h in hs:
@@ -471,6 +476,13 @@ def run_batch(args, local):
             q = C.c_int64()
             _capi.check(L.gci_query(C.c_void_p(h), C.byref(q), None, None, None, None, None))
             nv.append(q.value)
+            if record:
+                tm = np.zeros(13)
+                _capi.check(L.gci_timings(C.c_void_p(h), _capi.ptr(tm), 13))
+                for i, nme in enumerate(phase_names):
+                    phase_sum[nme] += float(tm[i])
+                extra["macro_iterations"] += float(tm[10])
+                extra["rkpq_host_s"] += float(tm[11])
             L.gci_free(C.c_void_p(h))
         return tot, nv
 
@@ -488,7 +500,7 @@ def run_batch(args, local):
             hs = batch()
             torch.cuda.synchronize()
             t += time.perf_counter() - t0
-            fl, nv = stats_of(hs)
+            fl, nv = stats_of(hs, record=True)
     n1 = C.c_int64()
     _capi.check(L.gci_kernel_launches(C.byref(n1)))
     # the same molecules one gci_rkpq call after another (one stream)
@@ -511,7 +523,12 @@ def run_batch(args, local):
                        "l2": "flushed before every timed step"},
             "molecules_per_s": 64 * args.steps / t, "sequential_s": t_seq, "batch_s": t / args.steps,
             "speedup_vs_sequential": t_seq / (t / args.steps), "nvecs_total": int(sum(nv)),
-            "gpu_launches": int(n1.value - n0.value), "clocks": clk.summary()}
+            "gpu_launches": int(n1.value - n0.value), "clocks": clk.summary(),
+            "per_molecule_sums": {"device_phase_s": {k: v / args.steps for k, v in phase_sum.items()},
+                                  "macro_iterations": extra["macro_iterations"] / args.steps,
+                                  "gci_rkpq_wall_s": extra["rkpq_host_s"] / args.steps,
+                                  "definition": "sums over the 64 molecules of each handle's phase timers "
+                                                "(CUDA events on its worker's stream) and call wall time"}}
     print(json.dumps(line), flush=True)
 
 
@@ -735,11 +752,12 @@ def main():
             print(f"#  L1={a} L2={b} NT={c}  launches {int(n):5d}  {t:8.3f} s  {100 * t / max(tot, 1e-30):5.1f}%  "
                   f"{f / 1e12:8.2f} TF  {f / max(t, 1e-30) / 1e12:6.2f} TF/s", file=sys.stderr)
     if args.dump_work and rank == 0:
-        d = json.loads(WORK_FIXTURE.read_text()) if WORK_FIXTURE.exists() else {}
+        dump = Path(args.dump_work)
+        d = json.loads(dump.read_text()) if dump.exists() else {}
         d[args.config] = {"how": f"python bench.py --config {args.config} --dump-work on one B200 "
                                  f"(gci_stats of one job: GEMM flops and per-class ERI counters)",
                           "nvecs": int(state["nvecs"]), "stats": [float(x) for x in stats[-1]]}
-        WORK_FIXTURE.write_text(json.dumps(d, indent=1) + "\n")
+        dump.write_text(json.dumps(d, indent=1) + "\n")
     fl = flops.job_flops(stats[-1], "lib")
     flops_step = fl["total"]
     sec = t_max / args.steps

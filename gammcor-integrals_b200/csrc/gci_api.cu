@@ -1093,11 +1093,13 @@ static void step1(Handle& H)
         CU(cudaStreamSynchronize(s));
     };
 
+    bool have_segmax = false;   // the candidates' maxima already read back with the last dmax
     while (go) {
         ++nmacro;
         // -------- chol2_DefineCandidates (:533-575)
         T.start(kCompress);
-        segment_max(cand);
+        if (!have_segmax) segment_max(cand);
+        have_segmax = false;
         std::vector<double> sv(segmax);
         std::vector<int64_t> si(cand);
         slatec_dsort(sv.data(), si.data(), (int64_t)si.size(), -2);
@@ -1139,9 +1141,10 @@ static void step1(Handle& H)
         int64_t maxnbatch = std::max<int64_t>((int64_t)maxnang * maxnang, 1000);
         if (maxnbatch > ncand) maxnbatch = ncand;
         const double dmin = std::max(0.01 * dmax, H.tau);
-        // -------- chol2_DefineBatch (:578-625)
-        segment_max(cand);
-        std::vector<double> dsv(segmax);
+        // -------- chol2_DefineBatch (:578-625).  Its per-pair maxima of D are those just
+        // sorted for the candidates (compression moves the values, it does not change
+        // them), so the list is re-sorted from the host copy as the reference re-sorts it
+        std::vector<double> dsv(sv.begin(), sv.begin() + (int64_t)cand.size());
         std::vector<int64_t> dsi(cand);
         slatec_dsort(dsv.data(), dsi.data(), (int64_t)dsi.size(), -2);
         std::vector<int64_t> batch, colloc;
@@ -1221,15 +1224,16 @@ static void step1(Handle& H)
             dpiv.ensure(nbatch);
             dpdmax.ensure(nbatch);
             CU(launch_pivot_batch(dMbb.p, (int)nbatch, dDb.p, dLb.p, dpiv.p, dpdmax.p, dnpiv.p, nchol, maxnchol, dmin, s));
+            // the pivot count and the batch-length pivot lists in one read-back
             int npiv = 0;
+            std::vector<int> piv(nbatch);
+            std::vector<double> pdm(nbatch);
             CU(cudaMemcpyAsync(&npiv, dnpiv.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CU(cudaMemcpyAsync(piv.data(), dpiv.p, sizeof(int) * nbatch, cudaMemcpyDeviceToHost, s));
+            CU(cudaMemcpyAsync(pdm.data(), dpdmax.p, sizeof(double) * nbatch, cudaMemcpyDeviceToHost, s));
             CU(cudaStreamSynchronize(s));
-            std::vector<int> piv(npiv);
-            std::vector<double> pdm(npiv);
-            if (npiv > 0) {
-                CU(cudaMemcpyAsync(piv.data(), dpiv.p, sizeof(int) * npiv, cudaMemcpyDeviceToHost, s));
-                CU(cudaMemcpyAsync(pdm.data(), dpdmax.p, sizeof(double) * npiv, cudaMemcpyDeviceToHost, s));
-            }
+            piv.resize(npiv);
+            pdm.resize(npiv);
             if (npiv > 0) {
                 // vectors over all candidates: L_new Lp^T = M(:, piv), solved by forward
                 // substitution (the column-by-column recursion of chol2_Lj,
@@ -1256,7 +1260,6 @@ static void step1(Handle& H)
                 }
             }
             T.stop();
-            CU(cudaStreamSynchronize(s));
             for (int j = 0; j < npiv; ++j) {
                 const int64_t full = bfull[piv[j]];
                 H.pivots[full] = 1;
@@ -1267,7 +1270,9 @@ static void step1(Handle& H)
         }
         CU(launch_max(dD.p, ncand, dscal.p, s));
         CU(cudaMemcpyAsync(&dmax, dscal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
-        CU(cudaStreamSynchronize(s));
+        // the next DefineCandidates' maxima come back with dmax (segment_max synchronises)
+        segment_max(cand);
+        have_segmax = true;
         T.flush();
         if (ncand == 0) dmax = -1e300;
         if (trace) {
