@@ -608,6 +608,7 @@ def run_dense(args):
     t_ours = timed(ours_trsm) - timed(lambda: B.copy_(B0))
     t_lib = timed(lambda: torch.linalg.solve_triangular(Lp, B0, upper=False))
     ref = torch.linalg.solve_triangular(Lp, B0, upper=False)
+    ours_trsm()   # the timing of the copy above left B = B0
     out[f"trsm_rlt {rows}x{w}"] = {"ours_s": t_ours, "cublas_trsm_s": t_lib, "max_abs_diff": float((B - ref).abs().max())}
     print(json.dumps({"dense_kernels": out, "note": "wall time around each call with a device synchronisation; "
                       "the library calls include their argument checks and stream synchronisation"}), flush=True)
