@@ -337,6 +337,17 @@ def mixed_vs_fp64(L, bstruct, c_dev, nao, a0, a1, b0, b1, buffer_mb, state, torc
     return out
 
 
+def virtual_ranges(nvecs: int, na: int, b0: int, b1: int, free_bytes: float, frac: float = 0.55):
+    """Split the virtual orbitals b0..b1 (1-based, inclusive) into the fewest equal ranges
+    whose Rkab block (nvecs x na x range, FP64) fits in `frac` of the free device memory."""
+    nb = b1 - b0 + 1
+    nparts = 1
+    while nparts < nb and 8.0 * nvecs * na * -(-nb // nparts) > frac * free_bytes:
+        nparts += 1
+    width = -(-nb // nparts)
+    return [(q0, min(b1, q0 + width - 1)) for q0 in range(b0, b1 + 1, width)]
+
+
 def workload_name(config: str) -> str:
     from gammcor_integrals_b200 import molecules
     m = molecules.config(config)
@@ -693,12 +704,8 @@ def main():
             # (Inv_L, the integral chunks); otherwise in ranges of virtual orbitals, one
             # gci_rkab_device call each into the same buffer (c5: 48k vectors x 150 x 2700 =
             # 156 GB, more than the HBM and than 80% of the host memory of the box)
-            free = torch.cuda.mem_get_info()[0]
-            nparts = 1
-            while 8.0 * nv.value * NA * -(-NB // nparts) > 0.55 * free:
-                nparts += 1
-            nbp = -(-NB // nparts)
-            state["parts"] = [(b0 + q * nbp, min(b1, b0 + (q + 1) * nbp - 1)) for q in range(nparts)]
+            state["parts"] = virtual_ranges(nv.value, NA, b0, b1, torch.cuda.mem_get_info()[0])
+            nbp = max(q1 - q0 + 1 for q0, q1 in state["parts"])
             state["rkab"] = torch.empty(nv.value * NA * nbp, dtype=torch.float64, device="cuda")
             state["nvecs"] = nv.value
         for pb0, pb1 in state["parts"]:
